@@ -1,0 +1,202 @@
+/*
+ * fd2.h -- C ABI of the B200 (sm_100a) dose-calculation and fluence-optimization
+ * library.  Every entry point takes plain pointers, sizes and POD structs; device
+ * buffers are owned by the caller unless a handle says otherwise; streams are
+ * passed as `void*` (a cudaStream_t, NULL = legacy default stream).
+ *
+ * Return convention: 0 = success, negative = fd2_status error.  Nothing here
+ * calls exit().  The reference library returns bool with 1 = failure and exits
+ * the process on CUDA errors (FastDoseLib/include/helper_cuda.h:583-595); the C++
+ * compatibility shim (fd2_compat.hpp) maps status != 0 back to `return 1`.
+ *
+ * Thread safety: a context is used by one host thread at a time.  Handles made
+ * from a context must not be shared between contexts.
+ */
+#ifndef FD2_H
+#define FD2_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum fd2_status {
+    FD2_OK = 0,
+    FD2_ERR_INVALID_ARGUMENT = -1,
+    FD2_ERR_CUDA = -2,
+    FD2_ERR_OUT_OF_MEMORY = -3,
+    FD2_ERR_IO = -4,
+    FD2_ERR_GEOMETRY = -5,      /* beam misses the bounding box, canonical beamlet fit failed */
+    FD2_ERR_CAPACITY = -6,      /* a caller-provided buffer is too small */
+    FD2_ERR_WATCHDOG = -7,      /* a bounded device loop hit its iteration cap */
+    FD2_ERR_NOT_SUPPORTED = -8,
+    FD2_ERR_ADMISSION = -9      /* request does not fit the HBM admission budget */
+} fd2_status;
+
+/* Human-readable name of a status code (static storage). */
+const char* fd2_status_string(int status);
+/* ABI version: major*10000 + minor*100 + patch. */
+int fd2_version(void);
+/* Last error message recorded on this host thread (static per-thread storage). */
+const char* fd2_last_error(void);
+
+/* ------------------------------------------------------------------ beams */
+/*
+ * Beam / beamlet descriptor.  Byte-for-byte the layout of fastdose::d_BEAM_d
+ * (FastDoseLib/include/beam.cuh:84-133: float3 isocenter, float2 beamlet_size,
+ * uint2 fmap_size, float sad, float3 angles, float long_spacing, float lim_min,
+ * float lim_max, uint long_dim, float3 source, size_t TermaBEV_pitch,
+ * size_t DensityBEV_pitch), so an existing device array of d_BEAM_d can be
+ * passed unchanged.  96 bytes; the two pad words are the alignment gaps the
+ * CUDA vector types leave.
+ *   angles = (gantry theta, couch phi, collimator) in radians.
+ *   pitches are in bytes; this library requires Terma/Density/Dose pitches equal.
+ */
+typedef struct fd2_beam {
+    float isocenter[3];
+    uint32_t pad0;
+    float beamlet_size[2];
+    uint32_t fmap_size[2];
+    float sad;
+    float angles[3];
+    float long_spacing;
+    float lim_min;
+    float lim_max;
+    uint32_t long_dim;
+    float source[3];
+    uint32_t pad1;
+    uint64_t TermaBEV_pitch;
+    uint64_t DensityBEV_pitch;
+} fd2_beam_t;
+
+/* Volume geometry: density is float[z][y][x], x fastest (reference density.cuh:12). */
+typedef struct fd2_volume {
+    uint32_t dim[3];         /* VolumeDim (x, y, z) */
+    float voxel_size[3];     /* cm */
+    uint32_t bbox_start[3];  /* BBoxStart, voxels */
+    uint32_t bbox_dim[3];    /* BBoxDim, voxels */
+} fd2_volume_t;
+
+/*
+ * BEAM_h::calc_range (FastDoseLib/src/beam.cu:134-222): source position,
+ * [lim_min, lim_max] and long_dim of one beam against the volume bounding box.
+ * Host-only, single precision with the reference's operation order.
+ * Reads isocenter, beamlet_size, fmap_size, sad, angles, long_spacing;
+ * writes source, lim_min, lim_max, long_dim.
+ */
+int fd2_beam_calc_range(fd2_beam_t* beam, const fd2_volume_t* volume);
+
+/* Beam-bundle parameters, the IMRT::BeamBundle fields (IMRTOpt/include/IMRTBeamBundle.cuh:9-31). */
+typedef struct fd2_bundle {
+    float isocenter[3];
+    float beamlet_size[2];
+    int32_t fluence_dim[2];
+    float sad;
+    float angles[3];
+    float long_spacing;
+    int32_t sub_fluence_dim[2];
+    int32_t sub_fluence_on[2];
+} fd2_bundle_t;
+
+/*
+ * IMRT::BeamBundle::beamletInit (IMRTOpt/src/IMRTBeamBundle.cu:341-569): the
+ * canonical sub-beam of fluence pixel (ix, iy) of a bundle, with calc_range
+ * applied.  Host-only, single precision.  Fluence of the sub-beam is the centred
+ * sub_fluence_on^2 open square of a sub_fluence_dim^2 map (fd2_beamlet_fluence).
+ */
+int fd2_beamlet_init(const fd2_bundle_t* bundle, int ix, int iy,
+                     const fd2_volume_t* volume, fd2_beam_t* out);
+
+/* Writes the sub-beam fluence map (float[fy][fx]) of a bundle into `out`. */
+int fd2_beamlet_fluence(const fd2_bundle_t* bundle, float* out, size_t n);
+
+/* ------------------------------------------------------------------ context */
+typedef struct fd2_context fd2_context;
+typedef struct fd2_density fd2_density;
+typedef struct fd2_spectrum fd2_spectrum;
+typedef struct fd2_cccs_kernel fd2_cccs_kernel;
+typedef struct fd2_csr_ensemble fd2_csr_ensemble;
+
+/* Creates a context on CUDA device `device` (makes it current on this thread). */
+int fd2_context_create(int device, fd2_context** out);
+int fd2_context_destroy(fd2_context* ctx);
+/* Synchronises the context's internal streams. */
+int fd2_context_synchronize(fd2_context* ctx);
+
+/*
+ * fastdose::density_h2d (FastDoseLib/src/density.cu:23-58).  Copies a host
+ * density volume to the device.  Sampling is trilinear on texel centres i+0.5
+ * with zero outside the volume (the reference's linear/border texture).
+ */
+int fd2_density_create(fd2_context* ctx, const float* host_density,
+                       const fd2_volume_t* volume, fd2_density** out);
+int fd2_density_destroy(fd2_density* d);
+/* Device pointer of the density volume (float[z][y][x]). */
+const float* fd2_density_device_ptr(const fd2_density* d);
+
+/*
+ * SPECTRUM_h::bind_spectrum (FastDoseLib/src/TermaComp.cu:67-78).  `fluence`
+ * is the normalised bin weight as read_spectrum_file leaves it
+ * (spectrum.cu:41-42).  n <= 24 (MAX_KERNEL_NUM).  The table lives in the handle,
+ * not in process-global constant memory, so several spectra can coexist.
+ */
+int fd2_spectrum_create(fd2_context* ctx, int n, const float* energy, const float* fluence,
+                        const float* mu, const float* mu_en, fd2_spectrum** out);
+int fd2_spectrum_destroy(fd2_spectrum* s);
+
+/*
+ * KERNEL_h::bind_kernel (FastDoseLib/src/DoseComp.cu:25-38).  theta is the bin
+ * middle angle; phi the azimuths.  nTheta, nPhi <= 24.
+ */
+int fd2_kernel_create(fd2_context* ctx, int n_theta, const float* theta,
+                      const float* A, const float* a, const float* B, const float* b,
+                      int n_phi, const float* phi, fd2_cccs_kernel** out);
+int fd2_kernel_destroy(fd2_cccs_kernel* k);
+
+/* ------------------------------------------------------------------ dose calc */
+/*
+ * fastdose::TermaComputeCollective (FastDoseLib/src/TermaComp.cu:153-176).
+ * d_beams: device array of n_beams descriptors.  d_fluence / d_terma /
+ * d_density_bev: device arrays of n_beams device pointers (the reference's
+ * float** convention).  Outputs are [long_dim][pitch/4] per beam.
+ */
+int fd2_terma_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_beams,
+                      const fd2_beam_t* d_beams, float* const* d_fluence,
+                      float* const* d_terma, float* const* d_density_bev,
+                      const fd2_density* density, const fd2_spectrum* spectrum,
+                      void* stream);
+
+/*
+ * fastdose::DoseComputeCollective (FastDoseLib/src/DoseComp.cu:179-214).
+ * Accumulates (+=) into d_dose like the reference; zero it first for a fresh beam.
+ */
+int fd2_dose_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_beams,
+                     const fd2_beam_t* d_beams, float* const* d_terma,
+                     float* const* d_density_bev, float* const* d_dose,
+                     const fd2_cccs_kernel* kernel, void* stream);
+
+/*
+ * fastdose::BEV2PVCS (FastDoseLib/src/TermaComp.cu:97-150): one beam's BEV array
+ * d_bev ([long_dim][fmap_y][fmap_x], contiguous) resampled trilinearly onto the
+ * whole volume.  d_out is float[z][y][pitch/4].
+ */
+int fd2_bev2pvcs(fd2_context* ctx, const fd2_beam_t* h_beam, const fd2_density* density,
+                 const float* d_bev, float* d_out, size_t out_pitch_bytes, void* stream);
+
+/*
+ * fastdose::BEV2PVCS_SuperSampling (FastDoseLib/src/geom.cu:343-474).  Voxels
+ * farther than `extent` from the beam axis, or whose supersampled sum is below
+ * 1e-4, are left untouched, as in the reference.
+ */
+int fd2_bev2pvcs_supersampling(fd2_context* ctx, const fd2_beam_t* h_beam,
+                               const fd2_density* density, const float* d_bev,
+                               float* d_out, size_t out_pitch_bytes, int ssfactor,
+                               float extent, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FD2_H */
