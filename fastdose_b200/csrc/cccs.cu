@@ -1,0 +1,368 @@
+// cccs.cu -- collapsed-cone convolution/superposition in beam's-eye view.
+//
+// Restates d_DoseComputeCollective (FastDoseLib/src/DoseComp.cu:217-392).  For
+// every forward zenith bin theta (theta <= pi/2) and azimuth phi, the rays of
+// all BEV pixels -- translates of one base ray starting at (0.5, 0.5, 0) in
+// normalised BEV units -- march slice by slice through voxel boundaries.  Per
+// segment of path length p (physical, with divergence) in voxel v:
+//     dose[v] += (A/a * XA + B/b * XB) * p * rho[v]       (g == 1, quirk Q1)
+//     sum_p[v] += p * rho[v]
+//     X <- T[v] (1 - e^{-k p rho}) + e^{-k p rho} X          for (k, X) in {(a, XA), (b, XB)}
+// with lateral wrap-around and the recursion reset on crossing an edge (Q4).
+// After all azimuths of a slice, dose_bev[s] += sum_phi dose / (sum_p_lastphi + 1e-4)
+// (Q2: the path sum of the last azimuth only).
+//
+// B200 design.  The reference runs one block per beamlet with one thread per
+// pixel and a block barrier after every ray step, azimuths in sequence.  Here a
+// block owns one beamlet (schedule 0: all zenith bins in turn) or one
+// (beamlet, zenith bin) (schedule 1), and each WARP owns one azimuth: its 32
+// lanes carry all P rays (P/32 independent recursions per lane, which the
+// scheduler interleaves), every lane computes the shared base-ray step itself
+// (the warp stays converged, no broadcast), and the only barriers are the
+// three per slice that stage the slice's Terma/density pair into shared memory
+// and reduce the azimuths.  Within one step the rays of a beamlet deposit into
+// distinct voxels (a shift permutation), so the warp-private deposit buffer
+// needs only a __syncwarp between steps.
+//
+// Boundary decisions (next voxel boundary, slice snap, lateral wrap) use
+// correctly rounded float operations in the order the reference writes them,
+// starting from cone directions computed on the host; the CPU oracle performs
+// the identical operations, so both march the same segments bit for bit.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "fd2_internal.cuh"
+
+namespace fd2 {
+
+namespace {
+
+constexpr int kStepCap = 1 << 20;  // per-slice step cap (the watchdog bound)
+
+struct RayGeom {  // per-beamlet scalars the march needs
+    float hx, hy;      // fmap_size / 2
+    float bsx, bsy;    // beamlet_size
+    float ls, lim_min, inv_sad;
+    float ffx, ffy;    // fmap size as float
+    int fx, fy, P, L;
+};
+
+__device__ __forceinline__ float step_to_boundary(float c, float d) {
+    // (ceil(c + 1e-3) - c) / d for d > 0, (floor(c - 1e-3) - c) / d otherwise,
+    // with the reference's fast division (its build uses -use_fast_math, whose
+    // a/b is bitwise __fdividef(a, b)).  An axis the ray does not move along
+    // never limits the step (the reference divides by zero there and the ray
+    // becomes NaN and never ends its slice).
+    if (d == 0.0f) return __int_as_float(0x7f800000);
+    return d > 0.0f ? __fdividef(__fsub_rn(ceilf(__fadd_rn(c, 1e-3f)), c), d)
+                    : __fdividef(__fsub_rn(floorf(__fsub_rn(c, 1e-3f)), c), d);
+}
+
+// d_nextPoint (DoseComp.cu:76-111): the next voxel-boundary point of the base ray.
+__device__ __forceinline__ bool next_point(float3 c, float3 d, float3& np) {
+    float sx = step_to_boundary(c.x, d.x), sy = step_to_boundary(c.y, d.y), sz = step_to_boundary(c.z, d.z);
+    float take = fminf(fminf(sx, sy), sz);
+    np = make_float3(__fmaf_rn(take, d.x, c.x), __fmaf_rn(take, d.y, c.y), __fmaf_rn(take, d.z, c.z));
+    bool flag = fabsf(__fsub_rn(np.z, roundf(np.z))) < 1e-4f;
+    if (flag) {
+        np = make_float3(__fmaf_rn(sz, d.x, c.x), __fmaf_rn(sz, d.y, c.y), roundf(__fmaf_rn(sz, d.z, c.z)));
+    }
+    return flag;
+}
+
+// Lateral voxel column of the segment midpoint (d_calcCoords, DoseComp.cu:147-164).
+__device__ __forceinline__ int mid_index(float b, float n, float ff, int f) {
+    float m = __fmul_rn(__fadd_rn(b, n), 0.5f);
+    float r = fmodf(m, ff);
+    r = r < 0.0f ? __fadd_rn(r, ff) : r;
+    int i = (int)floorf(r);
+    return i < f ? i : f - 1;
+}
+
+__device__ __forceinline__ bool crosses_edge(float b, float n, float ff) {
+    return floorf(__fdividef(b, ff)) != floorf(__fdividef(n, ff));
+}
+
+// Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
+// the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
+// sums).  RPL = rays per lane (P <= 32 * RPL).
+template <int RPL>
+__global__ void __launch_bounds__(768) cccs_kernel(const fd2_beam_t* __restrict__ beams,
+                                                   const float* const* __restrict__ terma,
+                                                   const float* const* __restrict__ dens,
+                                                   float* const* __restrict__ dose,
+                                                   const float4* __restrict__ dirs,  // [beam][n_tf][n_phi]
+                                                   ConeParams cp, int split, float* __restrict__ split_out,
+                                                   size_t split_stride, DeviceStatus* status) {
+    extern __shared__ float2 smem[];
+    __shared__ int s_ctrl[2];  // next slice index, abort flag
+    int* s_next = &s_ctrl[0];
+    int* s_abort = &s_ctrl[1];
+    if (threadIdx.x == 0) *s_abort = 0;
+    const int n_tf = cp.n_theta_fwd, n_phi = cp.n_phi;
+    const int bi = split ? blockIdx.x / n_tf : blockIdx.x;
+    const int t0 = split ? blockIdx.x % n_tf : 0;
+    const int t1 = split ? t0 + 1 : n_tf;
+    const fd2_beam_t& b = beams[bi];
+    RayGeom g;
+    g.fx = b.fmap_size[0];
+    g.fy = b.fmap_size[1];
+    g.P = g.fx * g.fy;
+    g.L = (int)b.long_dim;
+    g.ffx = (float)g.fx;
+    g.ffy = (float)g.fy;
+    g.hx = g.fx * 0.5f;
+    g.hy = g.fy * 0.5f;
+    g.bsx = b.beamlet_size[0];
+    g.bsy = b.beamlet_size[1];
+    g.ls = b.long_spacing;
+    g.lim_min = b.lim_min;
+    g.inv_sad = 1.0f / b.sad;
+    const size_t pitch = b.TermaBEV_pitch / sizeof(float);
+
+    float2* tr = smem;
+    float2* dp = smem + g.P;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2* mydp = dp + (size_t)warp * g.P;
+    const float* __restrict__ T = terma[bi];
+    const float* __restrict__ R = dens[bi];
+    float* __restrict__ D = dose[bi];
+    const bool last_phi = warp == n_phi - 1;
+
+    // per-ray constant pixel coordinates
+    float fix[RPL], fiy[RPL];
+    bool act[RPL];
+#pragma unroll
+    for (int j = 0; j < RPL; j++) {
+        int r = j * 32 + lane;
+        act[j] = r < g.P;
+        fix[j] = (float)(r % g.fx);
+        fiy[j] = (float)(r / g.fx);
+    }
+
+    for (int t = t0; t < t1; t++) {
+        const float ka = cp.a[t], kb = cp.b[t], Aa = cp.A_a[t], Bb = cp.B_b[t];
+        const float4 d4 = dirs[((size_t)bi * n_tf + t) * n_phi + warp];
+        const float3 d = make_float3(d4.x, d4.y, d4.z);
+        float3 c = make_float3(0.5f, 0.5f, 0.0f);
+        float XA[RPL], XB[RPL];
+#pragma unroll
+        for (int j = 0; j < RPL; j++) XA[j] = XB[j] = 0.0f;
+
+        // The slice of every pass is the rounded z of the first azimuth's base
+        // ray (DoseComp.cu:300): when that ray ends a slice within 1e-3 below
+        // the next plane it steps over it, and the reference skips that slice
+        // for this zenith bin; the other azimuths keep marching from wherever
+        // they stopped.
+        if (threadIdx.x == 0) *s_next = 0;
+        __syncthreads();  // the previous pass has finished; s_next is visible
+        int s = *s_next;
+        while (s < g.L) {
+            for (int v = threadIdx.x; v < g.P; v += blockDim.x)
+                tr[v] = make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
+            for (int v = lane; v < g.P; v += 32) mydp[v] = make_float2(0.0f, 0.0f);
+            __syncthreads();
+
+            int guard = 0;
+            for (;;) {
+                float3 np;
+                const bool flag = next_point(c, d, np);
+                const float fe = (np.z * g.ls + g.lim_min) * g.inv_sad;
+                const float fs = (c.z * g.ls + g.lim_min) * g.inv_sad;
+                const float dzp = (np.z - c.z) * g.ls;
+#pragma unroll
+                for (int j = 0; j < RPL; j++) {
+                    const float btx = __fadd_rn(c.x, fix[j]), ntx = __fadd_rn(np.x, fix[j]);
+                    const float bty = __fadd_rn(c.y, fiy[j]), nty = __fadd_rn(np.y, fiy[j]);
+                    const int cx = mid_index(btx, ntx, g.ffx, g.fx);
+                    const int cy = mid_index(bty, nty, g.ffy, g.fy);
+                    const int mi = cx + cy * g.fx;
+                    const bool wrap = crosses_edge(btx, ntx, g.ffx) || crosses_edge(bty, nty, g.ffy);
+                    // physical segment length (d_calcLineSeg, DoseComp.cu:114-144)
+                    const float dxp = (ntx - g.hx) * g.bsx * fe - (btx - g.hx) * g.bsx * fs;
+                    const float dyp = (nty - g.hy) * g.bsy * fe - (bty - g.hy) * g.bsy * fs;
+                    const float l2 = dxp * dxp + dyp * dyp + dzp * dzp;
+                    const float len = l2 * rsqrtf(l2);
+                    const float2 trv = tr[act[j] ? mi : 0];
+                    const float p = len * trv.y;
+                    const float ea = __expf(-ka * p), eb = __expf(-kb * p);
+                    const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
+                    if (act[j]) {
+                        float2 acc = mydp[mi];
+                        acc.x += dep;
+                        acc.y += p;
+                        mydp[mi] = acc;
+                    }
+                    XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
+                    XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
+                }
+                c = np;
+                __syncwarp();
+                if (flag) break;
+                if (++guard >= kStepCap) {
+                    if (lane == 0) {
+                        atomicExch(&status->code, (int)FD2_ERR_WATCHDOG);
+                        *s_abort = 1;
+                    }
+                    break;
+                }
+            }
+            if (threadIdx.x == 0) {
+                // the first azimuth's plane after this slice; it always lies ahead
+                const int nxt = (int)roundf(c.z);
+                *s_next = nxt > s ? nxt : g.L;
+            }
+            __syncthreads();
+            const int s_new = *s_abort ? g.L : *s_next;
+            // reduce azimuths in order; normalise by the last azimuth's path sum
+            for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
+                float sum = 0.0f;
+                for (int w = 0; w < n_phi; w++) sum += dp[(size_t)w * g.P + v].x;
+                const float val = sum / (dp[(size_t)(n_phi - 1) * g.P + v].y + 1e-4f);
+                if (split)
+                    split_out[(size_t)blockIdx.x * split_stride + (size_t)s * g.P + v] = val;
+                else
+                    D[(size_t)s * pitch + v] += val;
+            }
+            __syncthreads();  // dp and tr are read; s_next was read by every thread
+            s = s_new;
+        }
+        (void)last_phi;
+    }
+}
+
+// dose_bev[s][v] += sum_t planes[t][s][v] (zenith bins in order)
+__global__ void cccs_split_reduce(const fd2_beam_t* __restrict__ beams, float* const* __restrict__ dose,
+                                  const float* __restrict__ planes, size_t stride, int n_tf) {
+    const int bi = blockIdx.y;
+    const fd2_beam_t& b = beams[bi];
+    const int P = b.fmap_size[0] * b.fmap_size[1];
+    const size_t n = (size_t)P * b.long_dim;
+    const size_t pitch = b.TermaBEV_pitch / sizeof(float);
+    float* D = dose[bi];
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        size_t s = i / P, v = i % P;
+        float acc = 0.0f;
+        for (int t = 0; t < n_tf; t++) acc += planes[((size_t)bi * n_tf + t) * stride + i];
+        D[s * pitch + v] += acc;
+    }
+}
+
+}  // namespace
+
+int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams, const fd2_beam_t* d_beams,
+                     const float* const* d_terma, const float* const* d_dens, float* const* d_dose,
+                     const fd2_cccs_kernel* k, int schedule, cudaStream_t stream) {
+    if (n_beams == 0) return FD2_OK;
+    ConeParams cp{};
+    std::vector<int> fwd;
+    for (int t = 0; t < k->n_theta; t++)
+        if ((double)k->theta[t] <= 1.5707963267948966) fwd.push_back(t);  // forward only, DoseComp.cu:265
+    if (fwd.empty()) return FD2_OK;
+    cp.n_theta_fwd = (int)fwd.size();
+    cp.n_phi = k->n_phi;
+    for (size_t i = 0; i < fwd.size(); i++) {
+        int t = fwd[i];
+        cp.a[i] = k->a[t];
+        cp.b[i] = k->b[t];
+        cp.A_a[i] = k->A[t] / k->a[t];
+        cp.B_b[i] = k->B[t] / k->b[t];
+    }
+    int maxP = 0, maxL = 0;
+    for (size_t i = 0; i < n_beams; i++) {
+        FD2_REQUIRE(h_beams[i].TermaBEV_pitch == h_beams[i].DensityBEV_pitch, FD2_ERR_INVALID_ARGUMENT,
+                    "dose_compute: Terma and density pitches differ");
+        maxP = std::max(maxP, (int)(h_beams[i].fmap_size[0] * h_beams[i].fmap_size[1]));
+        maxL = std::max(maxL, (int)h_beams[i].long_dim);
+    }
+    FD2_REQUIRE(maxP > 0 && maxP <= 1024, FD2_ERR_INVALID_ARGUMENT, "dose_compute: fmap of %d pixels (1..1024)", maxP);
+    // direction table [beam][theta_fwd][phi] as float4, evaluated on the device
+    ConeAngles ang{};
+    ang.n_theta_fwd = (int)fwd.size();
+    ang.n_phi = k->n_phi;
+    for (size_t t = 0; t < fwd.size(); t++) ang.theta[t] = k->theta[fwd[t]];
+    for (int f = 0; f < k->n_phi; f++) ang.phi[f] = k->phi[f];
+    size_t dir_bytes = n_beams * fwd.size() * k->n_phi * sizeof(float4);
+    size_t plane_stride = (size_t)maxP * maxL;
+    size_t plane_bytes = schedule == 1 ? n_beams * fwd.size() * plane_stride * sizeof(float) : 0;
+    void* scratch = nullptr;
+    FD2_TRY(ctx_scratch(ctx, dir_bytes + plane_bytes + 256, &scratch));
+    float4* d_dirs = (float4*)scratch;
+    float* d_planes = (float*)((char*)scratch + ((dir_bytes + 255) / 256) * 256);
+    FD2_TRY(launch_cone_dirs(d_beams, n_beams, ang, d_dirs, stream));
+    // slices a zenith pass skips must contribute zero
+    if (plane_bytes) FD2_CHECK_CUDA(cudaMemsetAsync(d_planes, 0, plane_bytes, stream));
+    const int threads = 32 * k->n_phi;
+    const size_t shm = (size_t)(1 + k->n_phi) * maxP * sizeof(float2);
+    const unsigned blocks = (unsigned)(schedule == 1 ? n_beams * fwd.size() : n_beams);
+    if (maxP <= 256) {
+        FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<8><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
+                                                         d_planes, plane_stride, ctx->d_status);
+    } else {
+        FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<32><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
+                                                          d_planes, plane_stride, ctx->d_status);
+    }
+    FD2_CHECK_CUDA(cudaGetLastError());
+    if (schedule == 1) {
+        dim3 grid(std::max(1, std::min(64, (int)((plane_stride + 255) / 256))), (unsigned)n_beams);
+        cccs_split_reduce<<<grid, 256, 0, stream>>>(d_beams, d_dose, d_planes, plane_stride, (int)fwd.size());
+        FD2_CHECK_CUDA(cudaGetLastError());
+    }
+    return FD2_OK;
+}
+
+// Automatic schedule: split the zenith bins across blocks when the beamlets
+// alone cannot fill the device (fewer than ~4 blocks per SM).
+int cccs_auto_schedule(const fd2_context* ctx, size_t n_beams) {
+    return n_beams < (size_t)ctx->sm_count * 4 ? 1 : 0;
+}
+
+}  // namespace fd2
+
+extern "C" int fd2_dose_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_beams, const fd2_beam_t* d_beams,
+                                float* const* d_terma, float* const* d_density_bev, float* const* d_dose,
+                                const fd2_cccs_kernel* kernel, void* stream) {
+    FD2_REQUIRE(ctx && d_beams && d_terma && d_density_bev && d_dose && kernel, FD2_ERR_INVALID_ARGUMENT,
+                "dose_compute: null argument");
+    FD2_REQUIRE(fmap_npixels > 0 && fmap_npixels <= 1024, FD2_ERR_INVALID_ARGUMENT,
+                "dose_compute: fmap_npixels %zu outside 1..1024", fmap_npixels);
+    if (n_beams == 0) return FD2_OK;
+    // the cone directions are evaluated on the host from the beam descriptors
+    std::vector<fd2_beam_t> hb(n_beams);
+    cudaStream_t st = (cudaStream_t)stream;
+    FD2_CHECK_CUDA(cudaMemcpyAsync(hb.data(), d_beams, n_beams * sizeof(fd2_beam_t), cudaMemcpyDeviceToHost, st));
+    FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+    return fd2::launch_cccs_host(ctx, n_beams, hb.data(), d_beams, (const float* const*)d_terma,
+                                 (const float* const*)d_density_bev, d_dose, kernel,
+                                 fd2::cccs_auto_schedule(ctx, n_beams), st);
+}
+
+extern "C" int fd2_cccs_cone_directions(fd2_context* ctx, const fd2_cccs_kernel* k, size_t n_beams,
+                                        const fd2_beam_t* h_beams, float* h_out, size_t n_out) {
+    FD2_REQUIRE(ctx && k && h_beams && h_out, FD2_ERR_INVALID_ARGUMENT, "cone_directions: null argument");
+    fd2::ConeAngles ang{};
+    for (int t = 0; t < k->n_theta; t++)
+        if ((double)k->theta[t] <= 1.5707963267948966) ang.theta[ang.n_theta_fwd++] = k->theta[t];
+    ang.n_phi = k->n_phi;
+    for (int f = 0; f < k->n_phi; f++) ang.phi[f] = k->phi[f];
+    const size_t n = n_beams * ang.n_theta_fwd * ang.n_phi;
+    FD2_REQUIRE(n_out >= 4 * n, FD2_ERR_CAPACITY, "cone_directions: need %zu floats", 4 * n);
+    if (!n) return FD2_OK;
+    fd2_beam_t* d_beams = nullptr;
+    float4* d_out = nullptr;
+    FD2_CHECK_CUDA(cudaMalloc(&d_beams, n_beams * sizeof(fd2_beam_t)));
+    cudaError_t e = cudaMalloc(&d_out, n * sizeof(float4));
+    if (e == cudaSuccess) e = cudaMemcpy(d_beams, h_beams, n_beams * sizeof(fd2_beam_t), cudaMemcpyHostToDevice);
+    int rc = FD2_OK;
+    if (e == cudaSuccess) rc = fd2::launch_cone_dirs(d_beams, n_beams, ang, d_out, ctx->stream);
+    if (e == cudaSuccess && rc == FD2_OK) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess && rc == FD2_OK) e = cudaMemcpy(h_out, d_out, n * sizeof(float4), cudaMemcpyDeviceToHost);
+    cudaFree(d_beams);
+    if (d_out) cudaFree(d_out);
+    if (rc) return rc;
+    FD2_CHECK_CUDA(e);
+    return FD2_OK;
+}

@@ -1,0 +1,151 @@
+// context.cu -- context, density, spectrum and CCCS-kernel handles.
+#include <cstring>
+
+#include "fd2_internal.cuh"
+
+namespace fd2 {
+
+int ctx_scratch(fd2_context* ctx, size_t bytes, void** out) {
+    if (bytes > ctx->scratch_bytes) {
+        if (ctx->scratch) FD2_CHECK_CUDA(cudaFree(ctx->scratch));
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+        FD2_CHECK_CUDA(cudaMalloc(&ctx->scratch, bytes));
+        ctx->scratch_bytes = bytes;
+    }
+    *out = ctx->scratch;
+    return FD2_OK;
+}
+
+}  // namespace fd2
+
+extern "C" {
+
+int fd2_context_create(int device, fd2_context** out) {
+    FD2_REQUIRE(out, FD2_ERR_INVALID_ARGUMENT, "context_create: null out");
+    *out = nullptr;
+    int n = 0;
+    FD2_CHECK_CUDA(cudaGetDeviceCount(&n));
+    FD2_REQUIRE(device >= 0 && device < n, FD2_ERR_INVALID_ARGUMENT, "no CUDA device %d (%d present)", device, n);
+    FD2_CHECK_CUDA(cudaSetDevice(device));
+    auto* c = new fd2_context();
+    c->device = device;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) {
+        delete c;
+        fd2::set_error("cudaGetDeviceProperties failed");
+        return FD2_ERR_CUDA;
+    }
+    c->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_status, sizeof(fd2::DeviceStatus)) != cudaSuccess ||
+        cudaMemset(c->d_status, 0, sizeof(fd2::DeviceStatus)) != cudaSuccess) {
+        fd2::set_error("context_create: stream/status allocation failed");
+        if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->d_status) cudaFree(c->d_status);
+        delete c;
+        return FD2_ERR_CUDA;
+    }
+    *out = c;
+    return FD2_OK;
+}
+
+int fd2_context_destroy(fd2_context* c) {
+    if (!c) return FD2_OK;
+    cudaSetDevice(c->device);
+    if (c->scratch) cudaFree(c->scratch);
+    if (c->d_status) cudaFree(c->d_status);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return FD2_OK;
+}
+
+int fd2_context_synchronize(fd2_context* c) {
+    FD2_REQUIRE(c, FD2_ERR_INVALID_ARGUMENT, "null context");
+    FD2_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    return FD2_OK;
+}
+
+int fd2_density_create(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume, fd2_density** out) {
+    FD2_REQUIRE(ctx && host_density && volume && out, FD2_ERR_INVALID_ARGUMENT, "density_create: null argument");
+    size_t nv = (size_t)volume->dim[0] * volume->dim[1] * volume->dim[2];
+    FD2_REQUIRE(nv > 0, FD2_ERR_INVALID_ARGUMENT, "density_create: empty volume");
+    FD2_REQUIRE(volume->voxel_size[0] > 0 && volume->voxel_size[1] > 0 && volume->voxel_size[2] > 0,
+                FD2_ERR_INVALID_ARGUMENT, "density_create: voxel size must be positive");
+    auto* d = new fd2_density();
+    d->ctx = ctx;
+    d->vol = *volume;
+    if (cudaMalloc(&d->d_density, nv * sizeof(float)) != cudaSuccess) {
+        delete d;
+        fd2::set_error("density_create: cudaMalloc of %zu bytes failed", nv * sizeof(float));
+        return FD2_ERR_OUT_OF_MEMORY;
+    }
+    if (cudaMemcpy(d->d_density, host_density, nv * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d->d_density);
+        delete d;
+        fd2::set_error("density_create: copy failed");
+        return FD2_ERR_CUDA;
+    }
+    *out = d;
+    return FD2_OK;
+}
+
+int fd2_density_destroy(fd2_density* d) {
+    if (!d) return FD2_OK;
+    if (d->d_density) cudaFree(d->d_density);
+    delete d;
+    return FD2_OK;
+}
+
+const float* fd2_density_device_ptr(const fd2_density* d) { return d ? d->d_density : nullptr; }
+
+int fd2_spectrum_create(fd2_context* ctx, int n, const float* energy, const float* fluence, const float* mu,
+                        const float* mu_en, fd2_spectrum** out) {
+    FD2_REQUIRE(ctx && energy && fluence && mu && out, FD2_ERR_INVALID_ARGUMENT, "spectrum_create: null argument");
+    FD2_REQUIRE(n > 0 && n <= fd2::kMaxSpectrum, FD2_ERR_INVALID_ARGUMENT,
+                "spectrum_create: %d bins (1..%d supported, MAX_KERNEL_NUM)", n, fd2::kMaxSpectrum);
+    auto* s = new fd2_spectrum();
+    s->ctx = ctx;
+    s->n = n;
+    for (int i = 0; i < n; i++) {
+        s->energy[i] = energy[i];
+        s->fluence[i] = fluence[i];
+        s->mu[i] = mu[i];
+        s->mu_en[i] = mu_en ? mu_en[i] : 0.0f;
+    }
+    *out = s;
+    return FD2_OK;
+}
+
+int fd2_spectrum_destroy(fd2_spectrum* s) {
+    delete s;
+    return FD2_OK;
+}
+
+int fd2_kernel_create(fd2_context* ctx, int n_theta, const float* theta, const float* A, const float* a,
+                      const float* B, const float* b, int n_phi, const float* phi, fd2_cccs_kernel** out) {
+    FD2_REQUIRE(ctx && theta && A && a && B && b && phi && out, FD2_ERR_INVALID_ARGUMENT,
+                "kernel_create: null argument");
+    FD2_REQUIRE(n_theta > 0 && n_theta <= fd2::kMaxAngles && n_phi > 0 && n_phi <= fd2::kMaxAngles,
+                FD2_ERR_INVALID_ARGUMENT, "kernel_create: nTheta=%d nPhi=%d (1..%d supported)", n_theta, n_phi,
+                fd2::kMaxAngles);
+    for (int i = 0; i < n_theta; i++)
+        FD2_REQUIRE(a[i] > 0 && b[i] > 0, FD2_ERR_INVALID_ARGUMENT, "kernel_create: a and b must be positive");
+    auto* k = new fd2_cccs_kernel();
+    k->ctx = ctx;
+    k->n_theta = n_theta;
+    k->n_phi = n_phi;
+    for (int i = 0; i < n_theta; i++) {
+        k->theta[i] = theta[i]; k->A[i] = A[i]; k->a[i] = a[i]; k->B[i] = B[i]; k->b[i] = b[i];
+    }
+    for (int i = 0; i < n_phi; i++) k->phi[i] = phi[i];
+    *out = k;
+    return FD2_OK;
+}
+
+int fd2_kernel_destroy(fd2_cccs_kernel* k) {
+    delete k;
+    return FD2_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,630 @@
+// dosemat.cu -- dose-loading-matrix construction (IMRT::DoseMatConstruction,
+// IMRTOpt/src/IMRTDoseMat.cu:14-301), the CSR ensemble with its on-disk layout
+// (IMRT::MatCSREnsemble, IMRTOpt/src/IMRTSparseMatEns.cu), BEV->PVCS entry points
+// and beamlet flagging (IMRT::beamletFlagInit, IMRTOpt/src/IMRTBeamBundle.cu:130-316).
+//
+// Pipeline per batch of beamlets (a batch holds whole beams and is sized by a
+// BEV-scratch memory budget instead of the reference's one beam per iteration):
+//   Terma (one launch) -> CCCS (one launch) -> column count -> column values
+//   -> row gather into the growing device CSR.
+// Two small device->host reads per batch (row capacities, row nnz) size the
+// buffers; there is no dense beamlets x voxels matrix.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <string>
+#include <sys/stat.h>
+#include <vector>
+
+#include "fd2_internal.cuh"
+#include "resample.cuh"
+
+struct fd2_csr_ensemble {
+    fd2_context* ctx = nullptr;
+    uint64_t n_cols = 0;
+    int value_type = FD2_VALUES_F32;
+    std::vector<uint64_t> mat_rows;  // [n_mats + 1]
+    uint64_t n_rows = 0, nnz = 0;
+    int64_t* d_row_off = nullptr;    // [n_rows + 1]
+    int32_t* d_col = nullptr;        // [cap]
+    void* d_val = nullptr;           // [cap]
+    float* d_scale = nullptr;        // [n_rows] (16-bit formats)
+    uint64_t row_cap = 0, nnz_cap = 0;
+};
+
+namespace fd2 {
+
+namespace {
+
+size_t value_bytes(int vt) { return vt == FD2_VALUES_F32 ? 4 : 2; }
+
+void rot_axis_d(const double p[3], const double r[3], double t, double o[3]) {
+    double s = std::sin(t), c = std::cos(t);
+    double k = (1 - c) * (p[0] * r[0] + p[1] * r[1] + p[2] * r[2]);
+    double a = k * r[0] + c * p[0] + s * (r[1] * p[2] - r[2] * p[1]);
+    double b = k * r[1] + c * p[1] + s * (r[2] * p[0] - r[0] * p[2]);
+    double d = k * r[2] + c * p[2] + s * (r[0] * p[1] - r[1] * p[0]);
+    o[0] = a; o[1] = b; o[2] = d;
+}
+
+// Grows the ensemble's device arrays (amortised doubling).
+int ensemble_reserve(fd2_csr_ensemble* e, uint64_t rows, uint64_t nnz) {
+    if (rows + 1 > e->row_cap) {
+        uint64_t cap = std::max<uint64_t>(rows + 1, e->row_cap * 2);
+        int64_t* p;
+        FD2_CHECK_CUDA(cudaMalloc(&p, cap * sizeof(int64_t)));
+        if (e->d_row_off) {
+            FD2_CHECK_CUDA(cudaMemcpy(p, e->d_row_off, (e->n_rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice));
+            cudaFree(e->d_row_off);
+        } else {
+            FD2_CHECK_CUDA(cudaMemset(p, 0, sizeof(int64_t)));
+        }
+        e->d_row_off = p;
+        if (e->value_type != FD2_VALUES_F32) {
+            float* s;
+            FD2_CHECK_CUDA(cudaMalloc(&s, cap * sizeof(float)));
+            if (e->d_scale) {
+                FD2_CHECK_CUDA(cudaMemcpy(s, e->d_scale, e->n_rows * sizeof(float), cudaMemcpyDeviceToDevice));
+                cudaFree(e->d_scale);
+            }
+            e->d_scale = s;
+        }
+        e->row_cap = cap;
+    }
+    if (nnz > e->nnz_cap) {
+        uint64_t cap = std::max<uint64_t>(nnz, e->nnz_cap + e->nnz_cap / 2);
+        int32_t* c;
+        void* v;
+        FD2_CHECK_CUDA(cudaMalloc(&c, cap * sizeof(int32_t)));
+        FD2_CHECK_CUDA(cudaMalloc(&v, cap * value_bytes(e->value_type)));
+        if (e->d_col) {
+            FD2_CHECK_CUDA(cudaMemcpy(c, e->d_col, e->nnz * sizeof(int32_t), cudaMemcpyDeviceToDevice));
+            FD2_CHECK_CUDA(cudaMemcpy(v, e->d_val, e->nnz * value_bytes(e->value_type), cudaMemcpyDeviceToDevice));
+            cudaFree(e->d_col);
+            cudaFree(e->d_val);
+        }
+        e->d_col = c;
+        e->d_val = v;
+        e->nnz_cap = cap;
+    }
+    return FD2_OK;
+}
+
+template <typename T>
+int upload(const std::vector<T>& h, T** d, cudaStream_t st) {
+    FD2_CHECK_CUDA(cudaMallocAsync((void**)d, std::max<size_t>(1, h.size()) * sizeof(T), st));
+    if (!h.empty()) FD2_CHECK_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return FD2_OK;
+}
+
+}  // namespace
+
+void make_column_info(const fd2_beam_t& b, const fd2_volume_t* vol, ColumnInfo& ci) {
+    std::memset(&ci, 0, sizeof(ci));
+    // PVCS -> BEV (rotateBeamAtOriginRHS, FastDoseLib/src/geom.cu:36-44) applied to unit vectors
+    const double th = b.angles[0], ph = b.angles[1], co = b.angles[2];
+    const double axis[3] = {std::sin(-ph), 0.0, std::cos(-ph)}, yax[3] = {0, 1, 0};
+    for (int c = 0; c < 3; c++) {
+        double e[3] = {0, 0, 0}, t[3], o[3];
+        e[c] = 1;
+        rot_axis_d(e, axis, -th, t);
+        rot_axis_d(t, yax, ph + co, o);
+        for (int r = 0; r < 3; r++) ci.R[r * 3 + c] = (float)o[r];
+    }
+    for (int i = 0; i < 3; i++) ci.src[i] = b.source[i];
+    ci.bsx = b.beamlet_size[0];
+    ci.bsy = b.beamlet_size[1];
+    ci.fx = (int)b.fmap_size[0];
+    ci.fy = (int)b.fmap_size[1];
+    ci.hx = 0.5f * ci.fx;
+    ci.hy = 0.5f * ci.fy;
+    ci.inv_sad = 1.0f / b.sad;
+    ci.lim_min = b.lim_min;
+    ci.ls = b.long_spacing;
+    ci.inv_ls = 1.0f / b.long_spacing;
+    ci.L = (int)b.long_dim;
+    if (!vol) return;
+    // frustum corners in BEV (x lateral, y depth, z lateral) -> PVCS box
+    const double vx = vol->voxel_size[0], vy = vol->voxel_size[1], vz = vol->voxel_size[2];
+    const double hdiag = 0.5 * std::sqrt(vx * vx + vy * vy + vz * vz);
+    const double y0 = std::max(1e-3, (double)b.lim_min - hdiag), y1 = (double)b.lim_min + ci.L * (double)ci.ls + hdiag;
+    double lo[3] = {1e30, 1e30, 1e30}, hi[3] = {-1e30, -1e30, -1e30};
+    for (int k = 0; k < 8; k++) {
+        double y = (k & 1) ? y1 : y0;
+        double x = ((k & 2) ? 1 : -1) * (ci.hx * ci.bsx * y / b.sad);
+        double z = ((k & 4) ? 1 : -1) * (ci.hy * ci.bsy * y / b.sad);
+        // BEV -> PVCS is the transpose of R
+        for (int r = 0; r < 3; r++) {
+            double p = ci.R[0 * 3 + r] * x + ci.R[1 * 3 + r] * y + ci.R[2 * 3 + r] * z + ci.src[r];
+            lo[r] = std::min(lo[r], p);
+            hi[r] = std::max(hi[r], p);
+        }
+    }
+    const double vsz[3] = {vx, vy, vz};
+    for (int r = 0; r < 3; r++) {
+        double a = (lo[r] - hdiag) / vsz[r] - 0.5, c = (hi[r] + hdiag) / vsz[r] - 0.5;
+        long i0 = (long)std::floor(a) - 1, i1 = (long)std::ceil(c) + 2;
+        i0 = std::max(0L, i0);
+        i1 = std::min((long)vol->dim[r], i1);
+        if (i1 < i0) i1 = i0;
+        ci.box[r] = (int)i0;
+        ci.box[3 + r] = (int)i1;
+    }
+}
+
+// Column emission of a batch of beamlets whose BEV dose is in `aD` (device
+// array of device pointers, [L][P] each): count -> values -> gather, appended
+// as rows to the ensemble.
+static int append_columns(fd2_csr_ensemble* e, const fd2_beam_t* hb, size_t nb, const float* const* aD,
+                          const fd2_volume_t& vol, float extent, int ss, cudaStream_t st) {
+    std::vector<ColumnInfo> infos(nb);
+    for (size_t k = 0; k < nb; k++) make_column_info(hb[k], &vol, infos[k]);
+    ColumnInfo* d_infos = nullptr;
+    uint32_t *d_cnt = nullptr, *d_nnz = nullptr;
+    uint64_t* d_cap_off = nullptr;
+    int64_t* d_roff = nullptr;
+    int32_t* d_tcol = nullptr;
+    float *d_tval = nullptr, *d_max = nullptr, *d_iscale = nullptr;
+    int rc = [&]() -> int {
+        FD2_TRY(upload(infos, &d_infos, st));
+        // row capacities: candidate voxels per beamlet
+        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_cnt, nb * sizeof(uint32_t), st));
+        FD2_TRY(launch_column_count(d_infos, nb, d_cnt, vol, extent, st));
+        std::vector<uint32_t> cnt(nb);
+        FD2_CHECK_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+        std::vector<uint64_t> cap(nb + 1, 0);
+        for (size_t k = 0; k < nb; k++) cap[k + 1] = cap[k] + cnt[k];
+        FD2_TRY(upload(cap, &d_cap_off, st));
+        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_tcol, std::max<uint64_t>(1, cap[nb]) * sizeof(int32_t), st));
+        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_tval, std::max<uint64_t>(1, cap[nb]) * sizeof(float), st));
+        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_nnz, nb * sizeof(uint32_t), st));
+        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_max, nb * sizeof(float), st));
+        FD2_TRY(launch_column_values(d_infos, nb, aD, d_cap_off, d_tcol, d_tval, d_nnz, d_max, vol, extent, ss, st));
+        std::vector<uint32_t> nnz(nb);
+        std::vector<float> vmax(nb);
+        FD2_CHECK_CUDA(cudaMemcpyAsync(nnz.data(), d_nnz, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        FD2_CHECK_CUDA(cudaMemcpyAsync(vmax.data(), d_max, nb * sizeof(float), cudaMemcpyDeviceToHost, st));
+        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+        // final row offsets of this batch, appended to the ensemble
+        std::vector<int64_t> roff(nb + 1);
+        roff[0] = (int64_t)e->nnz;
+        for (size_t k = 0; k < nb; k++) {
+            FD2_REQUIRE(nnz[k] <= cnt[k], FD2_ERR_CAPACITY, "column overflow (internal)");
+            roff[k + 1] = roff[k] + nnz[k];
+        }
+        FD2_TRY(ensemble_reserve(e, e->n_rows + nb, (uint64_t)roff[nb]));
+        FD2_CHECK_CUDA(cudaMemcpyAsync(e->d_row_off + e->n_rows + 1, roff.data() + 1, nb * sizeof(int64_t),
+                                       cudaMemcpyHostToDevice, st));
+        FD2_TRY(upload(roff, &d_roff, st));
+        if (e->value_type != FD2_VALUES_F32) {
+            // per-row scale: the row maximum maps to 1 (value = scale * stored)
+            std::vector<float> sc(nb), isc(nb);
+            for (size_t k = 0; k < nb; k++) {
+                sc[k] = vmax[k] > 0 ? vmax[k] : 1.0f;
+                isc[k] = 1.0f / sc[k];
+            }
+            FD2_CHECK_CUDA(
+                cudaMemcpyAsync(e->d_scale + e->n_rows, sc.data(), nb * sizeof(float), cudaMemcpyHostToDevice, st));
+            FD2_TRY(upload(isc, &d_iscale, st));
+        }
+        FD2_TRY(launch_column_gather(nb, d_cap_off, d_roff, d_tcol, d_tval, d_iscale, e->d_col, e->d_val,
+                                     e->value_type, st));
+        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+        e->n_rows += nb;
+        e->nnz = (uint64_t)roff[nb];
+        return FD2_OK;
+    }();
+    for (void* p : {(void*)d_infos, (void*)d_cnt, (void*)d_nnz, (void*)d_cap_off, (void*)d_roff, (void*)d_tcol,
+                    (void*)d_tval, (void*)d_max, (void*)d_iscale})
+        if (p) cudaFreeAsync(p, st);
+    return rc;
+}
+
+}  // namespace fd2
+
+using namespace fd2;
+
+extern "C" {
+
+void fd2_dosemat_params_default(fd2_dosemat_params_t* p) {
+    if (!p) return;
+    p->extent = 2.0f;       // IMRTOpt/src/IMRTArgs.cpp:60
+    p->ss_factor = 5;       // IMRTOpt/src/IMRTgeom.cu:352
+    p->value_type = FD2_VALUES_F32;
+    p->cccs_schedule = -1;
+    p->batch_beamlets = 0;
+    p->memory_budget = 0;
+    p->verbose = 0;
+}
+
+int fd2_bev2pvcs(fd2_context* ctx, const fd2_beam_t* h_beam, const fd2_density* density, const float* d_bev,
+                 float* d_out, size_t out_pitch_bytes, void* stream) {
+    FD2_REQUIRE(ctx && h_beam && density && d_bev && d_out, FD2_ERR_INVALID_ARGUMENT, "bev2pvcs: null argument");
+    FD2_REQUIRE(out_pitch_bytes >= density->vol.dim[0] * sizeof(float) && out_pitch_bytes % sizeof(float) == 0,
+                FD2_ERR_INVALID_ARGUMENT, "bev2pvcs: bad pitch");
+    ColumnInfo ci;
+    make_column_info(*h_beam, nullptr, ci);
+    return launch_bev2pvcs(ci, density->vol, d_bev, d_out, out_pitch_bytes / sizeof(float), 0, 0.0f,
+                           (cudaStream_t)stream);
+}
+
+int fd2_bev2pvcs_supersampling(fd2_context* ctx, const fd2_beam_t* h_beam, const fd2_density* density,
+                               const float* d_bev, float* d_out, size_t out_pitch_bytes, int ssfactor, float extent,
+                               void* stream) {
+    FD2_REQUIRE(ctx && h_beam && density && d_bev && d_out, FD2_ERR_INVALID_ARGUMENT, "bev2pvcs: null argument");
+    FD2_REQUIRE(ssfactor > 0 && ssfactor <= 16, FD2_ERR_INVALID_ARGUMENT, "bev2pvcs: ssfactor %d", ssfactor);
+    FD2_REQUIRE(out_pitch_bytes >= density->vol.dim[0] * sizeof(float) && out_pitch_bytes % sizeof(float) == 0,
+                FD2_ERR_INVALID_ARGUMENT, "bev2pvcs: bad pitch");
+    ColumnInfo ci;
+    make_column_info(*h_beam, nullptr, ci);
+    return launch_bev2pvcs(ci, density->vol, d_bev, d_out, out_pitch_bytes / sizeof(float), ssfactor, extent,
+                           (cudaStream_t)stream);
+}
+
+int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_per_beam, const fd2_beam_t* h_beamlets,
+                           const float* h_fluence, const fd2_density* density, const fd2_spectrum* spectrum,
+                           const fd2_cccs_kernel* kernel, const fd2_dosemat_params_t* params_in,
+                           fd2_csr_ensemble** out, void* stream) {
+    FD2_REQUIRE(ctx && n_per_beam && h_beamlets && h_fluence && density && spectrum && kernel && out,
+                FD2_ERR_INVALID_ARGUMENT, "dose_mat_construct: null argument");
+    *out = nullptr;
+    fd2_dosemat_params_t params;
+    fd2_dosemat_params_default(&params);
+    if (params_in) params = *params_in;
+    FD2_REQUIRE(params.ss_factor > 0 && params.ss_factor <= 16, FD2_ERR_INVALID_ARGUMENT, "ss_factor out of range");
+    FD2_REQUIRE(params.value_type >= 0 && params.value_type <= 2, FD2_ERR_INVALID_ARGUMENT, "bad value type");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    const fd2_volume_t& vol = density->vol;
+    const uint64_t nvox = (uint64_t)vol.dim[0] * vol.dim[1] * vol.dim[2];
+    FD2_REQUIRE(nvox < (1ull << 31), FD2_ERR_NOT_SUPPORTED, "volume of %llu voxels exceeds int32 column indices",
+                (unsigned long long)nvox);
+
+    size_t total = 0;
+    for (size_t i = 0; i < n_beams; i++) total += n_per_beam[i];
+    const uint32_t fx = total ? h_beamlets[0].fmap_size[0] : 0, fy = total ? h_beamlets[0].fmap_size[1] : 0;
+    const size_t P = (size_t)fx * fy;
+    std::vector<fd2_beam_t> beams(h_beamlets, h_beamlets + total);
+    for (auto& b : beams) {
+        FD2_REQUIRE(b.fmap_size[0] == fx && b.fmap_size[1] == fy, FD2_ERR_INVALID_ARGUMENT,
+                    "dose_mat_construct: beamlets must share one fluence-map size");
+        FD2_REQUIRE(b.long_dim > 0 && b.sad > 0 && b.long_spacing > 0, FD2_ERR_INVALID_ARGUMENT,
+                    "dose_mat_construct: beamlet without a depth range (run calc_range)");
+        b.TermaBEV_pitch = b.DensityBEV_pitch = P * sizeof(float);
+    }
+    FD2_REQUIRE(P > 0 || total == 0, FD2_ERR_INVALID_ARGUMENT, "empty fluence map");
+    FD2_REQUIRE(P <= 1024, FD2_ERR_NOT_SUPPORTED, "fluence map of %zu pixels (max 1024)", P);
+
+    auto* e = new fd2_csr_ensemble();
+    e->ctx = ctx;
+    e->n_cols = nvox;
+    e->value_type = params.value_type;
+    e->mat_rows.assign(1, 0);
+    int rc = ensemble_reserve(e, 0, 0);
+    if (rc) { fd2_csr_ensemble_destroy(e); return rc; }
+
+    // memory budget for the BEV scratch of one batch
+    size_t free_b = 0, tot_b = 0;
+    cudaMemGetInfo(&free_b, &tot_b);
+    size_t budget = params.memory_budget ? params.memory_budget : std::min<size_t>(free_b / 4, (size_t)16 << 30);
+
+    float* d_fluence = nullptr;
+    fd2_beam_t* d_beams = nullptr;
+    rc = upload(std::vector<float>(h_fluence, h_fluence + P), &d_fluence, st);
+    if (!rc) rc = upload(beams, &d_beams, st);
+
+    size_t b0 = 0, beam0 = 0;
+    while (!rc && beam0 < n_beams) {
+        // whole beams into the batch while the scratch fits
+        size_t beam1 = beam0, b1 = b0, bytes = 0;
+        while (beam1 < n_beams) {
+            size_t add = 0;
+            for (size_t k = b1; k < b1 + n_per_beam[beam1]; k++) add += (size_t)beams[k].long_dim * P * 3 * sizeof(float);
+            size_t cnt = b1 + n_per_beam[beam1] - b0;
+            if (beam1 > beam0 && (bytes + add > budget || (params.batch_beamlets && cnt > params.batch_beamlets))) break;
+            bytes += add;
+            b1 += n_per_beam[beam1];
+            beam1++;
+        }
+        const size_t nb = b1 - b0;
+        if (nb == 0) {  // beams without beamlets
+            for (size_t i = beam0; i < beam1; i++) e->mat_rows.push_back(e->n_rows);
+            beam0 = beam1;
+            continue;
+        }
+        // BEV buffers [beamlet][L][P] for Terma, density, dose
+        std::vector<size_t> off(nb + 1, 0);
+        for (size_t k = 0; k < nb; k++) off[k + 1] = off[k] + (size_t)beams[b0 + k].long_dim * P;
+        float* d_bev = nullptr;
+        rc = [&]() -> int {
+            FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_bev, off[nb] * 3 * sizeof(float), st));
+            return FD2_OK;
+        }();
+        if (rc) break;
+        float *dT = d_bev, *dR = d_bev + off[nb], *dD = d_bev + 2 * off[nb];
+        std::vector<const float*> hF(nb, d_fluence);
+        std::vector<float*> hT(nb), hR(nb), hD(nb);
+        for (size_t k = 0; k < nb; k++) { hT[k] = dT + off[k]; hR[k] = dR + off[k]; hD[k] = dD + off[k]; }
+        const float** aF = nullptr;
+        float **aT = nullptr, **aR = nullptr, **aD = nullptr;
+        rc = [&]() -> int {
+            FD2_TRY(upload(hF, &aF, st));
+            FD2_TRY(upload(hT, &aT, st));
+            FD2_TRY(upload(hR, &aR, st));
+            FD2_TRY(upload(hD, &aD, st));
+            FD2_CHECK_CUDA(cudaMemsetAsync(dD, 0, off[nb] * sizeof(float), st));
+            FD2_TRY(launch_terma(ctx, P, nb, d_beams + b0, aF, aT, aR, density, spectrum, 1, st));
+            int sched = params.cccs_schedule >= 0 ? params.cccs_schedule : cccs_auto_schedule(ctx, nb);
+            FD2_TRY(launch_cccs_host(ctx, nb, beams.data() + b0, d_beams + b0, (const float* const*)aT,
+                                     (const float* const*)aR, aD, kernel, sched, st));
+            return append_columns(e, beams.data() + b0, nb, (const float* const*)aD, vol, params.extent,
+                                  params.ss_factor, st);
+        }();
+        // release batch buffers
+        for (void* p : {(void*)d_bev, (void*)aF, (void*)aT, (void*)aR, (void*)aD})
+            if (p) cudaFreeAsync(p, st);
+        if (rc) break;
+        // per-beam row boundaries
+        size_t row = e->n_rows - nb;
+        for (size_t i = beam0; i < beam1; i++) {
+            row += n_per_beam[i];
+            e->mat_rows.push_back(row);
+        }
+        if (params.verbose)
+            std::printf("dose matrix batch: beams %zu..%zu, %zu beamlets, nnz total %llu\n", beam0, beam1 - 1, nb,
+                        (unsigned long long)e->nnz);
+        b0 = b1;
+        beam0 = beam1;
+    }
+    if (d_fluence) cudaFreeAsync(d_fluence, st);
+    if (d_beams) cudaFreeAsync(d_beams, st);
+    cudaStreamSynchronize(st);
+    if (!rc) {
+        fd2::DeviceStatus ds;
+        if (cudaMemcpy(&ds, ctx->d_status, sizeof(ds), cudaMemcpyDeviceToHost) == cudaSuccess && ds.code != 0) {
+            cudaMemset(ctx->d_status, 0, sizeof(ds));
+            set_error("dose_mat_construct: a CCCS ray march hit its step cap");
+            rc = FD2_ERR_WATCHDOG;
+        }
+    }
+    if (rc) {
+        fd2_csr_ensemble_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return FD2_OK;
+}
+
+int fd2_bev2pvcs_interp(fd2_context* ctx, size_t n_beams, const uint32_t* n_per_beam, const fd2_beam_t* h_beamlets,
+                        const float* const* d_dose_bev, const fd2_density* density,
+                        const fd2_dosemat_params_t* params_in, fd2_csr_ensemble** out, void* stream) {
+    FD2_REQUIRE(ctx && n_per_beam && h_beamlets && d_dose_bev && density && out, FD2_ERR_INVALID_ARGUMENT,
+                "bev2pvcs_interp: null argument");
+    *out = nullptr;
+    fd2_dosemat_params_t params;
+    fd2_dosemat_params_default(&params);
+    if (params_in) params = *params_in;
+    FD2_REQUIRE(params.ss_factor > 0 && params.ss_factor <= 16, FD2_ERR_INVALID_ARGUMENT, "ss_factor out of range");
+    FD2_REQUIRE(params.value_type >= 0 && params.value_type <= 2, FD2_ERR_INVALID_ARGUMENT, "bad value type");
+    const fd2_volume_t& vol = density->vol;
+    const uint64_t nvox = (uint64_t)vol.dim[0] * vol.dim[1] * vol.dim[2];
+    FD2_REQUIRE(nvox < (1ull << 31), FD2_ERR_NOT_SUPPORTED, "volume exceeds int32 column indices");
+    cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+    auto* e = new fd2_csr_ensemble();
+    e->ctx = ctx;
+    e->n_cols = nvox;
+    e->value_type = params.value_type;
+    e->mat_rows.assign(1, 0);
+    int rc = ensemble_reserve(e, 0, 0);
+    size_t b0 = 0;
+    for (size_t i = 0; !rc && i < n_beams; i++) {
+        if (n_per_beam[i])
+            rc = append_columns(e, h_beamlets + b0, n_per_beam[i], d_dose_bev + b0, vol, params.extent,
+                                params.ss_factor, st);
+        b0 += n_per_beam[i];
+        e->mat_rows.push_back(e->n_rows);
+    }
+    if (rc) {
+        fd2_csr_ensemble_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_info(const fd2_csr_ensemble* e, fd2_csr_info_t* info) {
+    FD2_REQUIRE(e && info, FD2_ERR_INVALID_ARGUMENT, "ensemble_info: null argument");
+    info->n_mats = e->mat_rows.size() - 1;
+    info->n_rows = e->n_rows;
+    info->n_cols = e->n_cols;
+    info->nnz = e->nnz;
+    info->value_type = e->value_type;
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_device(const fd2_csr_ensemble* e, const int64_t** row_offsets, const int32_t** columns,
+                            const void** values, const float** row_scale, const uint64_t** mat_rows_host) {
+    FD2_REQUIRE(e, FD2_ERR_INVALID_ARGUMENT, "ensemble_device: null ensemble");
+    if (row_offsets) *row_offsets = e->d_row_off;
+    if (columns) *columns = e->d_col;
+    if (values) *values = e->d_val;
+    if (row_scale) *row_scale = e->d_scale;
+    if (mat_rows_host) *mat_rows_host = e->mat_rows.data();
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_to_host(const fd2_csr_ensemble* e, int64_t* row_offsets, int32_t* columns, float* values) {
+    FD2_REQUIRE(e, FD2_ERR_INVALID_ARGUMENT, "ensemble_to_host: null ensemble");
+    if (row_offsets)
+        FD2_CHECK_CUDA(cudaMemcpy(row_offsets, e->d_row_off, (e->n_rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    if (columns && e->nnz)
+        FD2_CHECK_CUDA(cudaMemcpy(columns, e->d_col, e->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (values && e->nnz) {
+        if (e->value_type == FD2_VALUES_F32) {
+            FD2_CHECK_CUDA(cudaMemcpy(values, e->d_val, e->nnz * sizeof(float), cudaMemcpyDeviceToHost));
+        } else {
+            std::vector<uint16_t> raw(e->nnz);
+            std::vector<float> sc(e->n_rows);
+            std::vector<int64_t> ro(e->n_rows + 1);
+            FD2_CHECK_CUDA(cudaMemcpy(raw.data(), e->d_val, e->nnz * 2, cudaMemcpyDeviceToHost));
+            FD2_CHECK_CUDA(cudaMemcpy(sc.data(), e->d_scale, e->n_rows * sizeof(float), cudaMemcpyDeviceToHost));
+            FD2_CHECK_CUDA(cudaMemcpy(ro.data(), e->d_row_off, (e->n_rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
+            for (uint64_t r = 0; r < e->n_rows; r++)
+                for (int64_t k = ro[r]; k < ro[r + 1]; k++) {
+                    float v;
+                    if (e->value_type == FD2_VALUES_F16) {
+                        __half h;
+                        std::memcpy(&h, &raw[k], 2);
+                        v = __half2float(h);
+                    } else {
+                        uint32_t bits = (uint32_t)raw[k] << 16;
+                        std::memcpy(&v, &bits, 4);
+                    }
+                    values[k] = v * sc[r];
+                }
+        }
+    }
+    return FD2_OK;
+}
+
+static int write_file(const std::string& path, const void* data, size_t bytes) {
+    std::ofstream f(path, std::ios::binary);
+    FD2_REQUIRE(f.is_open(), FD2_ERR_IO, "cannot open %s", path.c_str());
+    f.write((const char*)data, (std::streamsize)bytes);
+    FD2_REQUIRE(f.good(), FD2_ERR_IO, "write failed: %s", path.c_str());
+    return FD2_OK;
+}
+
+static int read_file(const std::string& path, std::vector<char>& out) {
+    std::ifstream f(path, std::ios::binary | std::ios::ate);
+    FD2_REQUIRE(f.is_open(), FD2_ERR_IO, "cannot open %s", path.c_str());
+    std::streamsize n = f.tellg();
+    f.seekg(0);
+    out.resize((size_t)n);
+    f.read(out.data(), n);
+    FD2_REQUIRE(f.good() || n == 0, FD2_ERR_IO, "read failed: %s", path.c_str());
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_tofile(const fd2_csr_ensemble* e, const char* folder) {
+    FD2_REQUIRE(e && folder, FD2_ERR_INVALID_ARGUMENT, "tofile: null argument");
+    mkdir(folder, 0755);
+    const std::string dir(folder);
+    const size_t nm = e->mat_rows.size() - 1;
+    std::vector<int64_t> ro(e->n_rows + 1);
+    FD2_CHECK_CUDA(cudaMemcpy(ro.data(), e->d_row_off, ro.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    std::vector<uint64_t> nnz(nm), cnnz(nm), nrows(nm), cnrows(nm), obi(nm);
+    std::vector<uint64_t> offsets;
+    offsets.reserve(e->n_rows + nm);
+    uint64_t obuf = 0;
+    for (size_t m = 0; m < nm; m++) {
+        uint64_t r0 = e->mat_rows[m], r1 = e->mat_rows[m + 1];
+        nnz[m] = (uint64_t)(ro[r1] - ro[r0]);
+        cnnz[m] = (m ? cnnz[m - 1] : 0) + nnz[m];
+        nrows[m] = r1 - r0;
+        cnrows[m] = (m ? cnrows[m - 1] : 0) + nrows[m];
+        obi[m] = obuf;
+        obuf += nrows[m] + 1;
+        for (uint64_t r = r0; r <= r1; r++) offsets.push_back((uint64_t)(ro[r] - ro[r0]));  // local offsets
+    }
+    FD2_TRY(write_file(dir + "/NonZeroElements.bin", nnz.data(), nm * 8));
+    FD2_TRY(write_file(dir + "/CumuNonZeroElements.bin", cnnz.data(), nm * 8));
+    FD2_TRY(write_file(dir + "/numRowsPerMat.bin", nrows.data(), nm * 8));
+    FD2_TRY(write_file(dir + "/CumuNumRowsPerMat.bin", cnrows.data(), nm * 8));
+    FD2_TRY(write_file(dir + "/OffsetBufferIdx.bin", obi.data(), nm * 8));
+    FD2_TRY(write_file(dir + "/offsetsBuffer.bin", offsets.data(), offsets.size() * 8));
+    std::vector<int32_t> col(e->nnz);
+    std::vector<float> val(e->nnz);
+    FD2_TRY(fd2_csr_ensemble_to_host(e, nullptr, col.data(), val.data()));
+    std::vector<uint64_t> col64(col.begin(), col.end());
+    FD2_TRY(write_file(dir + "/columnsBuffer.bin", col64.data(), col64.size() * 8));
+    FD2_TRY(write_file(dir + "/valuesBuffer.bin", val.data(), val.size() * 4));
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_cols, int value_type,
+                              fd2_csr_ensemble** out) {
+    FD2_REQUIRE(ctx && folder && out, FD2_ERR_INVALID_ARGUMENT, "fromfile: null argument");
+    FD2_REQUIRE(value_type == FD2_VALUES_F32, FD2_ERR_NOT_SUPPORTED, "fromfile: only F32 storage");
+    *out = nullptr;
+    const std::string dir(folder);
+    std::vector<char> b_nrows, b_off, b_col, b_val, b_nnz;
+    FD2_TRY(read_file(dir + "/numRowsPerMat.bin", b_nrows));
+    FD2_TRY(read_file(dir + "/NonZeroElements.bin", b_nnz));
+    FD2_TRY(read_file(dir + "/offsetsBuffer.bin", b_off));
+    FD2_TRY(read_file(dir + "/columnsBuffer.bin", b_col));
+    FD2_TRY(read_file(dir + "/valuesBuffer.bin", b_val));
+    const size_t nm = b_nrows.size() / 8;
+    FD2_REQUIRE(b_nnz.size() / 8 == nm, FD2_ERR_IO, "fromfile: NonZeroElements.bin has %zu entries, expected %zu",
+                b_nnz.size() / 8, nm);
+    const uint64_t* nrows = (const uint64_t*)b_nrows.data();
+    const uint64_t* off = (const uint64_t*)b_off.data();
+    const uint64_t* mnnz = (const uint64_t*)b_nnz.data();
+    const size_t nnz = b_col.size() / 8;
+    FD2_REQUIRE(b_val.size() / 4 == nnz, FD2_ERR_IO, "fromfile: values/columns size mismatch");
+    uint64_t total_rows = 0, check = 0;
+    for (size_t m = 0; m < nm; m++) { total_rows += nrows[m]; check += mnnz[m]; }
+    FD2_REQUIRE(check == nnz, FD2_ERR_IO, "fromfile: nnz mismatch");
+    FD2_REQUIRE(b_off.size() / 8 == total_rows + nm, FD2_ERR_IO, "fromfile: offsetsBuffer size mismatch");
+    std::vector<int64_t> ro(total_rows + 1, 0);
+    std::vector<uint64_t> mat_rows(1, 0);
+    size_t ob = 0, r = 0;
+    int64_t base = 0;
+    for (size_t m = 0; m < nm; m++) {
+        FD2_REQUIRE(off[ob] == 0 && off[ob + nrows[m]] == mnnz[m], FD2_ERR_IO, "fromfile: bad offsets of matrix %zu", m);
+        for (uint64_t k = 1; k <= nrows[m]; k++) {
+            FD2_REQUIRE(off[ob + k] >= off[ob + k - 1], FD2_ERR_IO, "fromfile: offsets not monotone");
+            ro[++r] = base + (int64_t)off[ob + k];
+        }
+        base += (int64_t)mnnz[m];
+        ob += nrows[m] + 1;
+        mat_rows.push_back(r);
+    }
+    const uint64_t* c64 = (const uint64_t*)b_col.data();
+    std::vector<int32_t> col(nnz);
+    for (size_t k = 0; k < nnz; k++) {
+        FD2_REQUIRE(c64[k] < n_cols, FD2_ERR_IO, "fromfile: column %llu out of range", (unsigned long long)c64[k]);
+        col[k] = (int32_t)c64[k];
+    }
+    auto* e = new fd2_csr_ensemble();
+    e->ctx = ctx;
+    e->n_cols = n_cols;
+    e->value_type = value_type;
+    e->mat_rows = mat_rows;
+    int rc = ensemble_reserve(e, total_rows, nnz);
+    if (!rc) {
+        cudaMemcpy(e->d_row_off, ro.data(), ro.size() * 8, cudaMemcpyHostToDevice);
+        if (nnz) {
+            cudaMemcpy(e->d_col, col.data(), nnz * 4, cudaMemcpyHostToDevice);
+            cudaMemcpy(e->d_val, b_val.data(), nnz * 4, cudaMemcpyHostToDevice);
+        }
+        e->n_rows = total_rows;
+        e->nnz = nnz;
+        if (cudaDeviceSynchronize() != cudaSuccess) rc = FD2_ERR_CUDA;
+    }
+    if (rc) {
+        fd2_csr_ensemble_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_destroy(fd2_csr_ensemble* e) {
+    if (!e) return FD2_OK;
+    if (e->d_row_off) cudaFree(e->d_row_off);
+    if (e->d_col) cudaFree(e->d_col);
+    if (e->d_val) cudaFree(e->d_val);
+    if (e->d_scale) cudaFree(e->d_scale);
+    delete e;
+    return FD2_OK;
+}
+
+int fd2_beamlet_flags_save(const uint8_t* flags, size_t n, const char* path) {
+    FD2_REQUIRE(flags && path, FD2_ERR_INVALID_ARGUMENT, "flags_save: null argument");
+    return write_file(path, flags, n);
+}
+
+}  // extern "C"

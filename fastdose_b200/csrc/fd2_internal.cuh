@@ -1,0 +1,131 @@
+// fd2_internal.cuh -- shared internals of libfd2 (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/fd2.h"
+#include "../../include/fd2_imrt.h"
+
+namespace fd2 {
+
+// ---------------------------------------------------------------- errors
+void set_error(const char* fmt, ...);
+
+#define FD2_CHECK_CUDA(call)                                                              \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            ::fd2::set_error("%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(e_)); \
+            return e_ == cudaErrorMemoryAllocation ? FD2_ERR_OUT_OF_MEMORY : FD2_ERR_CUDA;  \
+        }                                                                                  \
+    } while (0)
+
+#define FD2_REQUIRE(cond, code, ...)       \
+    do {                                   \
+        if (!(cond)) {                     \
+            ::fd2::set_error(__VA_ARGS__); \
+            return (code);                 \
+        }                                  \
+    } while (0)
+
+#define FD2_TRY(call)              \
+    do {                           \
+        int s_ = (call);           \
+        if (s_ != FD2_OK) return s_; \
+    } while (0)
+
+// Maximum table sizes, the reference's MAX_KERNEL_NUM / MAX_THETA_ANGLES
+// (FastDoseLib/include/spectrum.cuh:7, kernel.cuh:7).
+constexpr int kMaxSpectrum = 24;
+constexpr int kMaxAngles = 24;
+
+// Device-side status word written by kernels whose loops are bounded by an
+// iteration cap: 0 = fine, otherwise an FD2 status code (negative).
+struct DeviceStatus {
+    int code;
+    int where;
+};
+
+}  // namespace fd2
+
+// ---------------------------------------------------------------- handles
+struct fd2_context {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;          // internal work stream
+    fd2::DeviceStatus* d_status = nullptr;  // device status word
+    // reusable scratch, grown on demand
+    void* scratch = nullptr;
+    size_t scratch_bytes = 0;
+};
+
+struct fd2_density {
+    fd2_context* ctx = nullptr;
+    fd2_volume_t vol{};
+    float* d_density = nullptr;  // float[z][y][x]
+};
+
+struct fd2_spectrum {
+    fd2_context* ctx = nullptr;
+    int n = 0;
+    float energy[fd2::kMaxSpectrum];
+    float fluence[fd2::kMaxSpectrum];
+    float mu[fd2::kMaxSpectrum];
+    float mu_en[fd2::kMaxSpectrum];
+};
+
+struct fd2_cccs_kernel {
+    fd2_context* ctx = nullptr;
+    int n_theta = 0, n_phi = 0;
+    float theta[fd2::kMaxAngles], A[fd2::kMaxAngles], a[fd2::kMaxAngles], B[fd2::kMaxAngles],
+        b[fd2::kMaxAngles], phi[fd2::kMaxAngles];
+};
+
+namespace fd2 {
+
+// Scratch helper: returns a device buffer of at least `bytes` owned by ctx.
+int ctx_scratch(fd2_context* ctx, size_t bytes, void** out);
+
+// Spectrum table passed by value to kernels (lives in the kernel parameter
+// space, not in process-global __constant__ memory).
+struct SpectrumParams {
+    int n;
+    float fluence_energy_mu[kMaxSpectrum];  // fluence * energy * mu per bin
+    float mu[kMaxSpectrum];
+};
+
+// Per-cone constants of the CCCS march, one entry per (theta, phi) pair,
+// directions precomputed on the host (see cccs.cu).
+struct ConeParams {
+    int n_theta_fwd;        // forward zenith bins actually used
+    int n_phi;
+    float a[kMaxAngles], b[kMaxAngles];      // attenuation per used zenith bin
+    float A_a[kMaxAngles], B_b[kMaxAngles];  // A/a and B/b
+};
+
+// Forward zenith bins and azimuths of a CCCS kernel (the angles the cone
+// directions are made from).
+struct ConeAngles {
+    int n_theta_fwd;
+    int n_phi;
+    float theta[kMaxAngles];
+    float phi[kMaxAngles];
+};
+
+// Device table of cone directions, float4 [beam][theta_fwd][phi] (cccs_dirs.cu).
+int launch_cone_dirs(const fd2_beam_t* d_beams, size_t n_beams, const ConeAngles& ang, float4* d_out,
+                     cudaStream_t stream);
+
+// Launchers used by the plan-level code (dosemat.cu).
+int launch_terma(fd2_context* ctx, size_t fmap_npixels, size_t n_beams, const fd2_beam_t* d_beams,
+                 const float* const* d_fluence, float* const* d_terma, float* const* d_dens,
+                 const fd2_density* density, const fd2_spectrum* spectrum, int fluence_skip,
+                 cudaStream_t stream);
+
+}  // namespace fd2

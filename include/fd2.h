@@ -21,6 +21,9 @@
 #ifdef __cplusplus
 extern "C" {
 #endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
 
 /* ------------------------------------------------------------------ status */
 typedef enum fd2_status {
@@ -179,6 +182,16 @@ int fd2_dose_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_beams,
                      const fd2_cccs_kernel* kernel, void* stream);
 
 /*
+ * The cone directions the CCCS march uses: for every beam, forward zenith bin
+ * (theta <= pi/2) and azimuth, the unit direction in normalised BEV units,
+ * evaluated on the device with the reference's single-precision formula
+ * (FastDoseLib/src/DoseComp.cu:280-290).  h_out: float[n_beams][n_fwd][n_phi][4]
+ * (x, y, z, 0).  Diagnostic / test entry point.
+ */
+int fd2_cccs_cone_directions(fd2_context* ctx, const fd2_cccs_kernel* kernel, size_t n_beams,
+                             const fd2_beam_t* h_beams, float* h_out, size_t n_out);
+
+/*
  * fastdose::BEV2PVCS (FastDoseLib/src/TermaComp.cu:97-150): one beam's BEV array
  * d_bev ([long_dim][fmap_y][fmap_x], contiguous) resampled trilinearly onto the
  * whole volume.  d_out is float[z][y][pitch/4].
@@ -196,6 +209,9 @@ int fd2_bev2pvcs_supersampling(fd2_context* ctx, const fd2_beam_t* h_beam,
                                float* d_out, size_t out_pitch_bytes, int ssfactor,
                                float extent, void* stream);
 
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
 #ifdef __cplusplus
 }
 #endif

@@ -429,7 +429,9 @@ void or_terma(const fd2_beam_t* b, const float* fluence, const float* density,
 void or_next_point_f(const float c[3], const float d[3], float out[3], int* flag) {
     float st[3];
     for (int q = 0; q < 3; q++) {
-        if (d[q] > 0)
+        if (d[q] == 0.0f)
+            st[q] = INFINITY;  /* a still axis never limits the step */
+        else if (d[q] > 0)
             st[q] = (ceilf(c[q] + LARGER_EPS_FD) - c[q]) / d[q];
         else
             st[q] = (floorf(c[q] - LARGER_EPS_FD) - c[q]) / d[q];
@@ -484,7 +486,16 @@ void or_cone_direction(const fd2_beam_t* b, float theta, float phi, float out[3]
 void or_cccs(const fd2_beam_t* b, const float* terma, const float* dens, int n_theta,
              const float* theta, const float* A, const float* a, const float* B, const float* bb,
              int n_phi, const float* phi, float* dose) {
+    or_cccs_dirs(b, terma, dens, n_theta, theta, A, a, B, bb, n_phi, phi, NULL, dose);
+}
+
+/* As or_cccs; when `given` is not NULL it holds the cone directions
+ * [forward zenith bin][azimuth][4] to march with instead of or_cone_direction's. */
+void or_cccs_dirs(const fd2_beam_t* b, const float* terma, const float* dens, int n_theta,
+                  const float* theta, const float* A, const float* a, const float* B, const float* bb,
+                  int n_phi, const float* phi, const float* given, float* dose) {
     int fx = b->fmap_size[0], fy = b->fmap_size[1];
+    int t_fwd = 0;
     int P = fx * fy;
     size_t pitch = b->TermaBEV_pitch ? b->TermaBEV_pitch / sizeof(float) : (size_t)P;
     real* XA = (real*)calloc((size_t)n_phi * P, sizeof(real));
@@ -499,9 +510,15 @@ void or_cccs(const fd2_beam_t* b, const float* terma, const float* dens, int n_t
         memset(XA, 0, sizeof(real) * n_phi * P);
         memset(XB, 0, sizeof(real) * n_phi * P);
         for (int f = 0; f < n_phi; f++) {
-            or_cone_direction(b, theta[t], phi[f], dirs[f]);
+            if (given) {
+                const float* g = given + ((size_t)t_fwd * n_phi + f) * 4;
+                dirs[f][0] = g[0]; dirs[f][1] = g[1]; dirs[f][2] = g[2];
+            } else {
+                or_cone_direction(b, theta[t], phi[f], dirs[f]);
+            }
             base[f][0] = 0.5f; base[f][1] = 0.5f; base[f][2] = 0.0f;
         }
+        t_fwd++;
         for (;;) {
             int s = (int)roundf(base[0][2]);
             if (s >= (int)b->long_dim) break;

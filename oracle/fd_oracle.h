@@ -55,6 +55,12 @@ void or_terma(const fd2_beam_t* beam, const float* fluence, const float* density
 void or_cccs(const fd2_beam_t* beam, const float* terma, const float* dens, int n_theta,
              const float* theta, const float* A, const float* a, const float* B, const float* b,
              int n_phi, const float* phi, float* dose_io);
+/* As or_cccs, marching with the given cone directions
+ * ([forward zenith bin][azimuth][4], e.g. the library's device-evaluated table)
+ * instead of the double-precision ones; NULL selects the latter. */
+void or_cccs_dirs(const fd2_beam_t* beam, const float* terma, const float* dens, int n_theta,
+                  const float* theta, const float* A, const float* a, const float* B, const float* b,
+                  int n_phi, const float* phi, const float* dirs, float* dose_io);
 
 /* Dense BEV->PVCS linear resampling, TermaComp.cu:124-150.  out is [z][y][x]. */
 void or_bev2pvcs(const fd2_beam_t* beam, const float* bev, const fd2_volume_t* vol,

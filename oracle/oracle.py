@@ -147,14 +147,17 @@ def terma(beam, fluence, density, volume, spectrum, tex_mode=0, precision="doubl
     return T, R
 
 
-def cccs(beam, terma_bev, dens_bev, kernel, dose=None, precision="double"):
+def cccs(beam, terma_bev, dens_bev, kernel, dose=None, precision="double", dirs=None):
+    """CCCS of one beam.  `dirs` (optional, float32 [n_fwd][n_phi][4]) supplies
+    the cone directions; by default they are evaluated in double precision."""
     b = np.array(beam, BEAM_DTYPE).copy()
     L, fy, fx = _bev_shape(b)
     b["TermaBEV_pitch"] = b["DensityBEV_pitch"] = fx * fy * 4
     D = np.zeros((L, fy, fx), np.float32) if dose is None else np.ascontiguousarray(dose, np.float32).copy()
     k = kernel
-    lib(precision).or_cccs(_p(b), _p(_f32(terma_bev)), _p(_f32(dens_bev)), C.c_int(k.n_theta), _p(k.theta),
-                           _p(k.A), _p(k.a), _p(k.B), _p(k.b), C.c_int(k.n_phi), _p(k.phi), _p(D))
+    dp = _p(np.ascontiguousarray(dirs, np.float32)) if dirs is not None else None
+    lib(precision).or_cccs_dirs(_p(b), _p(_f32(terma_bev)), _p(_f32(dens_bev)), C.c_int(k.n_theta), _p(k.theta),
+                                _p(k.A), _p(k.a), _p(k.B), _p(k.b), C.c_int(k.n_phi), _p(k.phi), dp, _p(D))
     return D
 
 

@@ -242,8 +242,12 @@ int ref_dose_batch(int n, const fd2_beam_t* beams, const float* fluence, const f
             dim3 sgs{(vol->dim[0] - 1 + sbs.x) / sbs.x, (vol->dim[1] - 1 + sbs.y) / sbs.y,
                      (vol->dim[2] - 1 + sbs.z) / sbs.z};
             size_t preSize = (size_t)sgs.x * sgs.y * sgs.z * n;
+            // d_superVoxelInterp runs a 4^3-block grid that can exceed the
+            // supervoxel grid and then writes up to one padded grid past the
+            // array; allocate that slack so those writes stay in bounds.
+            size_t slack = (size_t)((sgs.x + 3) / 4 * 4) * ((sgs.y + 3) / 4 * 4) * ((sgs.z + 3) / 4 * 4);
             bool* pre;
-            cudaMalloc(&pre, preSize * sizeof(bool));
+            cudaMalloc(&pre, (preSize + slack) * sizeof(bool));
             int* longArr;
             cudaMalloc(&longArr, n * sizeof(int));
             std::vector<int> hl(n);

@@ -1,0 +1,163 @@
+"""Generates the dose-path golden fixtures by running the REFERENCE's own CUDA
+kernels (oracle/_ref/libfdref.so, built from the reference sources by
+oracle/build_ref.sh) on a GPU:
+
+  dose_c1_ref.npz     config 1 (64^3 slab phantom, 100 beamlets): Terma, density
+                      and dose BEV of four beamlets, their dose columns, the
+                      summed dose of all 100 columns, per-beamlet nnz, timings
+  dose_small_ref.npz  a small oblique case (all 16 beamlets)
+  bev2pvcs_ref.npz    fastdose::BEV2PVCS of one beamlet's dose (texture path)
+  flags_c2_ref.npz    beamletFlagInit of the 4pi torso bundles
+
+Usage (on a GPU machine): python tests/golden/make_golden_dose.py OUTDIR
+The fixtures are then copied next to this script.
+"""
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+from fastdose_b200 import phantoms  # noqa: E402
+from fastdose_b200.types import make_bundle  # noqa: E402
+from oracle import ref  # noqa: E402
+from plan_cases import c1_case, small_case  # noqa: E402
+
+PICK = [0, 44, 55, 93]
+
+
+def ref_kernel():
+    """The CCCS kernel used for every reference run: 8 zenith x 8 azimuth bins
+    (the reference's default nPhi, IMRTOpt/src/IMRTArgs.cpp:47).  With 6
+    azimuths one cone lies at phi = 90 degrees, where the reference's fast-math
+    direction has a zero component and its ray march divides by zero and never
+    finishes a slice; it is not run that way."""
+    return phantoms.synthetic_kernel(n_theta=8, n_phi=8)
+
+
+def log(*a):
+    print(*a, flush=True)
+
+
+def _csr_rows(dense, rows):
+    out = {}
+    for r in rows:
+        nz = np.nonzero(dense[r])[0]
+        out[f"col_{r}"] = nz.astype(np.int32)
+        out[f"val_{r}"] = dense[r, nz]
+    return out
+
+
+def c1(outdir):
+    case = c1_case()
+    cfg = case["cfg"]
+    ph = case["phantom"]
+    kern = ref_kernel()
+    log("c1: reference batch of", len(case["beams"]), "beamlets")
+    r = ref.dose_batch(case["beams"], case["fluence"], ph.density, ph.volume, cfg["spectrum"], kern,
+                       extent=cfg["extent"], dense=True, repeats=1)
+    assert r["status"] == 0, r["status"]
+    log("c1: done, timing")
+    # timing of the reference kernels on the same batch (three repeats)
+    t = ref.dose_batch(case["beams"], case["fluence"], ph.density, ph.volume, cfg["spectrum"], kern,
+                       extent=cfg["extent"], dense=True, repeats=3)["times_ms"]
+    log("c1: times", t)
+    dense = r["dense"]
+    keep = {}
+    for i in PICK:
+        L = int(case["beams"][i]["long_dim"])
+        keep[f"terma_{i}"] = r["terma"][i, :L]
+        keep[f"dens_{i}"] = r["dens"][i, :L]
+        keep[f"dose_{i}"] = r["dose"][i, :L]
+    nx, ny, nz = (int(v) for v in ph.volume["dim"])
+    np.savez_compressed(os.path.join(outdir, "dose_c1_ref.npz"), beams=case["beams"], pick=np.array(PICK),
+                        kernel_theta=kern.theta, kernel_A=kern.A, kernel_a=kern.a, kernel_B=kern.B,
+                        kernel_b=kern.b, kernel_phi=kern.phi,
+                        dose_sum=dense.sum(0).reshape(nz, ny, nx).astype(np.float32),
+                        nnz=(dense != 0).sum(1).astype(np.int64), times_ms=t, **keep, **_csr_rows(dense, PICK))
+    # dense trilinear resampling of beamlet 44's dose
+    b = case["beams"][44]
+    st, vol = ref.bev2pvcs(b, r["dose"][44, : int(b["long_dim"])], ph.volume)
+    assert st == 0
+    np.savez_compressed(os.path.join(outdir, "bev2pvcs_ref.npz"), beam=b, bev=r["dose"][44, : int(b["long_dim"])],
+                        out=vol)
+    return dict(c1_terma_ms=float(t[0]), c1_cccs_ms=float(t[1]), c1_interp_ms=float(t[2]),
+                c1_beamlets=int(len(case["beams"])))
+
+
+def small(outdir):
+    case = small_case()
+    ph = case["phantom"]
+    log("small: reference batch")
+    r = ref.dose_batch(case["beams"], case["fluence"], ph.density, ph.volume, case["spectrum"], case["kernel"],
+                       extent=2.0, dense=True)
+    assert r["status"] == 0
+    L = case["beams"]["long_dim"]
+    keep = {f"{k}_{i}": r[k][i, : int(L[i])] for k in ("terma", "dens", "dose") for i in range(len(L))}
+    np.savez_compressed(os.path.join(outdir, "dose_small_ref.npz"), beams=case["beams"], dense=r["dense"], **keep)
+
+
+def flags(outdir):
+    cfg = phantoms.config2()
+    ph = cfg["phantom"]
+    bundles = np.array([make_bundle(cfg["isocenter"], a, sad=cfg["sad"], fluence_dim=cfg["fluence_dim"],
+                                    beamlet_size=cfg["beamlet_size"], sub_fluence_dim=cfg["sub_fluence_dim"],
+                                    sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+                        for a in cfg["angles"]])
+    log("flags: reference beamletFlagInit of", len(bundles), "bundles")
+    st, fl = ref.beamlet_flags(bundles, ph.masks["PTV"], ph.volume, ph.density)
+    assert st == 0
+    np.savez_compressed(os.path.join(outdir, "flags_c2_ref.npz"), bundles=bundles, flags=fl)
+    return dict(c2_beams=int(len(bundles)), c2_active_beamlets=int(fl.sum()))
+
+
+def c2_timing(outdir, n_beams=8):
+    """Reference Terma + CCCS of whole 4pi beams (its interpolation stage is
+    not run on this volume: its supervoxel pass writes past its flag array when
+    the volume is not a multiple of 32 voxels)."""
+    cfg = phantoms.config2()
+    ph = cfg["phantom"]
+    fl = np.load(os.path.join(outdir, "flags_c2_ref.npz"))["flags"]
+    from fastdose_b200 import api
+
+    tot_b, tot_ms = 0, 0.0
+    for i in range(0, len(cfg["angles"]), max(1, len(cfg["angles"]) // n_beams))[:n_beams]:
+        bb = make_bundle(cfg["isocenter"], cfg["angles"][i], sad=cfg["sad"], fluence_dim=cfg["fluence_dim"],
+                         beamlet_size=cfg["beamlet_size"], sub_fluence_dim=cfg["sub_fluence_dim"],
+                         sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+        beams = api.bundle_beamlets(bb, fl[i], ph.volume)
+        if len(beams) == 0:
+            continue
+        log("c2 timing: beam", i, len(beams), "beamlets")
+        t = ref.dose_batch(beams, api.beamlet_fluence(bb), ph.density, ph.volume, cfg["spectrum"], ref_kernel(),
+                           dense=False, repeats=1)["times_ms"]
+        tot_b += len(beams)
+        tot_ms += float(t[0] + t[1])
+    return dict(c2_sample_beams=n_beams, c2_sample_beamlets=tot_b, c2_terma_cccs_ms=tot_ms,
+                c2_ref_beamlets_per_s=tot_b / (tot_ms * 1e-3) if tot_ms else None)
+
+
+def main():
+    outdir = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
+    os.makedirs(outdir, exist_ok=True)
+    if not ref.available():
+        raise SystemExit("oracle/_ref/libfdref.so missing: run oracle/build_ref.sh")
+    t0 = time.time()
+    meta = {}
+    meta.update(c1(outdir))
+    small(outdir)
+    meta.update(flags(outdir))
+    meta.update(c2_timing(outdir))
+    meta["wall_s"] = time.time() - t0
+    with open(os.path.join(outdir, "reference_timings.json"), "w") as f:
+        json.dump(meta, f, indent=1)
+    print(json.dumps(meta))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,173 @@
+"""CUDA dose path vs the CPU oracle: Terma, CCCS, BEV->PVCS, dose matrix.
+
+Each stage is fed the same inputs on both sides, so the comparison isolates
+that stage.  Tolerances: Terma and CCCS share every discrete decision with the
+oracle (same float boundary arithmetic), so only rounding of the physics
+differs (float vs double); the column stage point-samples, where a rounding
+flip moves one of ss^3 samples to a neighbouring texel.  The whole-plan check
+uses the dose tolerance of the parity gate: 0.5% of Dmax for the maximum
+difference and 0.1% of Dmax for the mean over voxels above 10% of Dmax.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from fastdose_b200 import api
+
+from plan_cases import c1_case, small_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(ctx, case, spectrum=None, kernel=None):
+    ph = case["phantom"]
+    spec = spectrum or case.get("spectrum") or case["cfg"]["spectrum"]
+    kern = kernel or case.get("kernel") or case["cfg"]["kernel"]
+    return (api.Density(ctx, ph.density, ph.volume), api.Spectrum(ctx, spec), api.Kernel(ctx, kern), spec, kern)
+
+
+def _run_bev(ctx, case, idx, schedule=None):
+    import torch
+
+    dens, sp, kn, spec, kern = _setup(ctx, case)
+    beams = case["beams"][idx]
+    batch = api.BEVBatch(beams)
+    api.TermaComputeCollective(ctx, batch, case["fluence"], dens, sp)
+    api.DoseComputeCollective(ctx, batch, kn)
+    torch.cuda.synchronize()
+    out = []
+    for i in range(len(beams)):
+        out.append((batch.get("terma", i).cpu().numpy(), batch.get("dens", i).cpu().numpy(),
+                    batch.get("dose", i).cpu().numpy()))
+    return batch.beams, out, spec, kern
+
+
+@pytest.mark.parametrize("case_fn,idx", [(small_case, [0, 5, 10, 15]), (c1_case, [0, 44, 93])])
+def test_terma_matches_oracle(ctx, case_fn, idx):
+    case = case_fn()
+    beams, out, spec, _ = _run_bev(ctx, case, idx)
+    for b, (T, R, _) in zip(beams, out):
+        To, Ro = oracle.terma(b, case["fluence"], case["phantom"].density, case["phantom"].volume, spec)
+        assert np.abs(T - To).max() <= 1e-4 * np.abs(To).max()
+        assert np.abs(R - Ro).max() <= 1e-4 * np.abs(Ro).max()
+
+
+@pytest.mark.parametrize("case_fn,idx", [(small_case, [0, 5, 10, 15]), (c1_case, [0, 44, 93])])
+def test_cccs_matches_oracle(ctx, case_fn, idx):
+    """The oracle marches with the device's cone directions; its boundary
+    arithmetic is correctly rounded where the kernel reproduces the
+    reference's fast division, so the two agree in the mean and up to the
+    march's floating-point sensitivity at isolated voxels."""
+    case = case_fn()
+    beams, out, _, kern = _run_bev(ctx, case, idx)
+    dirs = api.cone_directions(ctx, api.Kernel(ctx, kern), beams)
+    for i, (b, (T, R, D)) in enumerate(zip(beams, out)):
+        Do = oracle.cccs(b, T, R, kern, dirs=dirs[i])
+        assert np.abs(D - Do).mean() <= 5e-4 * np.abs(Do).max()
+        assert np.abs(D - Do).max() <= 5e-2 * np.abs(Do).max()
+
+
+def test_cccs_schedules_agree_bitwise(ctx):
+    import torch
+
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    res = []
+    for sched in (0, 1):
+        m = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn, cccs_schedule=sched)
+        res.append(m.to_host())
+    torch.cuda.synchronize()
+    for a, b in zip(*res):
+        np.testing.assert_array_equal(a, b)
+
+
+def _dense(ro, col, val, n_rows, n_cols):
+    out = np.zeros((n_rows, n_cols), np.float32)
+    for r in range(n_rows):
+        out[r, col[ro[r]:ro[r + 1]]] = val[ro[r]:ro[r + 1]]
+    return out
+
+
+def test_columns_match_oracle(ctx):
+    case = small_case()
+    beams, out, _, _ = _run_bev(ctx, case, list(range(16)))
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    m = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn)
+    ro, col, val = m.to_host()
+    nv = case["phantom"].density.size
+    A = _dense(ro, col, val, 16, nv)
+    for i, b in enumerate(beams):
+        row = oracle.beamlet_column(b, out[i][2], case["phantom"].volume)
+        mx = np.abs(row).max()
+        assert np.abs(A[i] - row).max() <= 0.01 * mx
+        assert np.abs(A[i] - row).mean() <= 1e-4 * mx
+        # same support except where the oracle value is within a sample flip of 0
+        diff = (A[i] != 0) != (row != 0)
+        assert np.all(np.abs(row[diff]) <= 0.01 * mx)
+
+
+def test_csr_structure_and_file_round_trip(ctx, tmp_path):
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    m = api.DoseMatConstruction(ctx, [case["beams"][:7], case["beams"][7:]], case["fluence"], dens, sp, kn)
+    info = m.info()
+    assert info["n_mats"] == 2 and info["n_rows"] == 16
+    ro, col, val = m.to_host()
+    assert ro[0] == 0 and np.all(np.diff(ro) >= 0) and ro[-1] == info["nnz"]
+    for r in range(16):
+        c = col[ro[r]:ro[r + 1]]
+        assert np.all(np.diff(c) > 0)
+        assert c.min() >= 0 and c.max() < info["n_cols"]
+    assert np.all(val != 0)
+    np.testing.assert_array_equal(m.mat_rows(), [0, 7, 16])
+    m.tofile(tmp_path)
+    # the reference layout: uint64 per-matrix arrays, local offsets, uint64 columns
+    nnz = np.fromfile(tmp_path / "NonZeroElements.bin", np.uint64)
+    np.testing.assert_array_equal(nnz, [ro[7] - ro[0], ro[16] - ro[7]])
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "CumuNonZeroElements.bin", np.uint64), np.cumsum(nnz))
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "numRowsPerMat.bin", np.uint64), [7, 9])
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "CumuNumRowsPerMat.bin", np.uint64), [7, 16])
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "OffsetBufferIdx.bin", np.uint64), [0, 8])
+    offs = np.fromfile(tmp_path / "offsetsBuffer.bin", np.uint64)
+    np.testing.assert_array_equal(offs[:8], ro[:8] - ro[0])
+    np.testing.assert_array_equal(offs[8:], ro[7:] - ro[7])
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "columnsBuffer.bin", np.uint64), col)
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "valuesBuffer.bin", np.float32), val)
+    m2 = api.MatCSREnsemble.fromfile(ctx, tmp_path, info["n_cols"])
+    for a, b in zip(m2.to_host(), (ro, col, val)):
+        np.testing.assert_array_equal(a, b)
+    np.testing.assert_array_equal(m2.mat_rows(), [0, 7, 16])
+
+
+@pytest.mark.parametrize("vt,rel", [("f16", 2 ** -11), ("bf16", 2 ** -8)])
+def test_half_precision_matrix(ctx, vt, rel):
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    ref = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn).to_host()
+    half = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn, value_type=vt)
+    ro, col, val = half.to_host()
+    np.testing.assert_array_equal(ro, ref[0])
+    np.testing.assert_array_equal(col, ref[1])
+    for r in range(len(ro) - 1):
+        a, b = val[ro[r]:ro[r + 1]], ref[2][ro[r]:ro[r + 1]]
+        assert np.abs(a - b).max() <= rel * np.abs(b).max() * 1.01
+
+
+def test_dose_matrix_c1_matches_oracle(ctx):
+    """Whole config-1 plan (100 beamlets, 6 azimuths) against the FP64 oracle:
+    the mean criterion of the parity gate; the maximum is bounded by the
+    march's floating-point sensitivity (see test_reference_parity.py)."""
+    case = c1_case()
+    dens, sp, kn, spec, kern = _setup(ctx, case)
+    m = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn)
+    ro, col, val = m.to_host()
+    nv = case["phantom"].density.size
+    gpu = np.zeros(nv, np.float64)
+    np.add.at(gpu, col, val)
+    rows = oracle.dose_rows(case["beams"], case["fluence"], case["phantom"].density, case["phantom"].volume, spec,
+                            kern, threads=8)
+    ref = rows.sum(0).astype(np.float64)
+    dmax = ref.max()
+    sel = ref > 0.1 * dmax
+    assert np.abs(gpu - ref).max() <= 5e-2 * dmax
+    assert np.abs(gpu - ref)[sel].mean() <= 1e-3 * dmax

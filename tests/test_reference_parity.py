@@ -1,0 +1,209 @@
+"""Parity against the REFERENCE's own CUDA output (golden fixtures made by
+tests/golden/make_golden_dose.py from the reference sources).
+
+The gate for the dose path: maximum difference within 0.5% of Dmax and mean
+difference within 0.1% of Dmax over voxels above 10% of Dmax.
+
+Why the CPU oracle is held to a looser maximum here: the reference's cone
+march makes discrete decisions (lateral wrap-around resets, the rule that
+skips a voxel boundary closer than 1e-3, the slice index taken from the first
+azimuth) on single-precision ray coordinates, and a one-ulp change of one
+azimuth moves a beamlet's dose by several percent of its maximum at isolated
+voxels.  The CUDA kernels reproduce the reference's floating-point operations
+for these decisions and meet the gate; the oracle restates them with
+correctly rounded arithmetic and agrees in the mean, not voxel for voxel.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from fastdose_b200 import api, phantoms
+from fastdose_b200.types import BUNDLE_DTYPE
+
+from plan_cases import c1_case, small_case
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+MAX_GATE, MEAN_GATE = 5e-3, 1e-3
+
+
+def _gold(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def _c1_kernel(g):
+    return phantoms.CCCSKernel(g["kernel_theta"], g["kernel_A"], g["kernel_a"], g["kernel_B"], g["kernel_b"],
+                               g["kernel_phi"])
+
+
+def _gate(test, ref, max_gate=MAX_GATE, mean_gate=MEAN_GATE):
+    ref = ref.astype(np.float64)
+    test = test.astype(np.float64)
+    dmax = ref.max()
+    sel = ref > 0.1 * dmax
+    dmx = np.abs(test - ref).max() / dmax
+    dmean = np.abs(test - ref)[sel].mean() / dmax
+    assert dmx <= max_gate, f"max diff {dmx:.3g} of Dmax"
+    assert dmean <= mean_gate, f"mean diff {dmean:.3g} of Dmax"
+    return dmx, dmean
+
+
+# ------------------------------------------------------------------ CPU: pin the oracle
+def test_oracle_terma_matches_reference():
+    g = _gold("dose_c1_ref.npz")
+    case = c1_case()
+    for i in g["pick"]:
+        T, R = oracle.terma(g["beams"][i], case["fluence"], case["phantom"].density, case["phantom"].volume,
+                            case["cfg"]["spectrum"], tex_mode=1)
+        # the reference samples density through the texture unit (8-bit weights)
+        assert np.abs(T - g[f"terma_{i}"]).max() <= 2e-3 * np.abs(g[f"terma_{i}"]).max()
+        assert np.abs(R - g[f"dens_{i}"]).max() <= 2e-3 * np.abs(g[f"dens_{i}"]).max()
+
+
+def test_oracle_cccs_matches_reference_in_the_mean():
+    g = _gold("dose_c1_ref.npz")
+    k = _c1_kernel(g)
+    maxes = []
+    for i in g["pick"]:
+        D = oracle.cccs(g["beams"][i], g[f"terma_{i}"], g[f"dens_{i}"], k)
+        ref = g[f"dose_{i}"]
+        maxes.append(np.abs(D - ref).max() / ref.max())
+        assert np.abs(D - ref).mean() <= 5e-4 * ref.max()
+    # isolated voxels carry the floating-point sensitivity of the march
+    assert max(maxes) <= 5e-2
+    # a beamlet whose march has no boundary-coincidence event matches closely
+    assert min(maxes) <= 1e-4
+
+
+def test_oracle_columns_match_reference():
+    g = _gold("dose_small_ref.npz")
+    case = small_case()
+    for i, b in enumerate(g["beams"]):
+        row = oracle.beamlet_column(b, g[f"dose_{i}"], case["phantom"].volume)
+        ref = g["dense"][i]
+        mx = np.abs(ref).max()
+        assert np.abs(row - ref).max() <= 0.02 * mx
+        assert np.abs(row - ref).mean() <= 2e-4 * mx
+
+
+# ------------------------------------------------------------------ GPU: the gate
+def _batch_from_golden(g, idx, fields=("terma", "dens")):
+    import torch
+
+    beams = g["beams"][idx]
+    batch = api.BEVBatch(beams)
+    for j, i in enumerate(idx):
+        L = int(beams[j]["long_dim"])
+        for f in fields:
+            batch.get(f, j).copy_(torch.from_numpy(np.ascontiguousarray(g[f"{f}_{i}"]).reshape(L, *batch.shape2)))
+    return batch
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("which", ["c1", "small"])
+def test_cccs_matches_reference(ctx, which):
+    import torch
+
+    if which == "c1":
+        g = _gold("dose_c1_ref.npz")
+        k = _c1_kernel(g)
+        idx = list(g["pick"])
+    else:
+        g = _gold("dose_small_ref.npz")
+        k = small_case()["kernel"]
+        idx = list(range(len(g["beams"])))
+    batch = _batch_from_golden(g, idx)
+    api.DoseComputeCollective(ctx, batch, api.Kernel(ctx, k))
+    torch.cuda.synchronize()
+    for j, i in enumerate(idx):
+        D = batch.get("dose", j).cpu().numpy()
+        ref = g[f"dose_{i}"].reshape(D.shape)
+        # same boundary decisions as the reference: far inside the gate
+        assert np.abs(D - ref).max() <= 1e-3 * ref.max()
+
+
+@pytest.mark.gpu
+def test_terma_matches_reference(ctx):
+    import torch
+
+    g = _gold("dose_c1_ref.npz")
+    case = c1_case()
+    idx = list(g["pick"])
+    batch = api.BEVBatch(g["beams"][idx])
+    dens = api.Density(ctx, case["phantom"].density, case["phantom"].volume)
+    api.TermaComputeCollective(ctx, batch, case["fluence"], dens, api.Spectrum(ctx, case["cfg"]["spectrum"]))
+    torch.cuda.synchronize()
+    for j, i in enumerate(idx):
+        T = batch.get("terma", j).cpu().numpy().reshape(g[f"terma_{i}"].shape)
+        R = batch.get("dens", j).cpu().numpy().reshape(g[f"dens_{i}"].shape)
+        assert np.abs(T - g[f"terma_{i}"]).max() <= 2e-3 * np.abs(g[f"terma_{i}"]).max()
+        assert np.abs(R - g[f"dens_{i}"]).max() <= 2e-3 * np.abs(g[f"dens_{i}"]).max()
+
+
+@pytest.mark.gpu
+def test_columns_match_reference(ctx):
+    g = _gold("dose_small_ref.npz")
+    case = small_case()
+    idx = list(range(len(g["beams"])))
+    batch = _batch_from_golden(g, idx, fields=("dose",))
+    dens = api.Density(ctx, case["phantom"].density, case["phantom"].volume)
+    m = api.BEV2PVCSInterp(ctx, batch, [len(idx)], dens)
+    ro, col, val = m.to_host()
+    for r in idx:
+        row = np.zeros(g["dense"].shape[1], np.float32)
+        row[col[ro[r]:ro[r + 1]]] = val[ro[r]:ro[r + 1]]
+        ref = g["dense"][r]
+        mx = np.abs(ref).max()
+        assert np.abs(row - ref).max() <= 0.02 * mx
+        assert np.abs(row - ref).mean() <= 2e-4 * mx
+    _gate(_dense_sum(ro, col, val, g), g["dense"].sum(0))
+
+
+def _dense_sum(ro, col, val, g):
+    out = np.zeros(g["dense"].shape[1], np.float64)
+    np.add.at(out, col, val)
+    return out
+
+
+@pytest.mark.gpu
+def test_bev2pvcs_dense_matches_reference(ctx):
+    import torch
+
+    g = _gold("bev2pvcs_ref.npz")
+    case = c1_case()
+    dens = api.Density(ctx, case["phantom"].density, case["phantom"].volume)
+    out = api.BEV2PVCS(ctx, g["beam"], dens, torch.from_numpy(np.ascontiguousarray(g["bev"])).cuda())
+    torch.cuda.synchronize()
+    out = out.cpu().numpy()
+    ref = g["out"]
+    # the reference interpolates through the texture unit (8-bit weights)
+    assert np.abs(out - ref).max() <= 5e-3 * np.abs(ref).max()
+
+
+@pytest.mark.gpu
+def test_beamlet_flags_match_reference(ctx):
+    g = _gold("flags_c2_ref.npz")
+    cfg = phantoms.config2()
+    ph = cfg["phantom"]
+    fl = api.beamletFlagInit(ctx, np.asarray(g["bundles"], BUNDLE_DTYPE), ph.masks["PTV"], ph.volume)
+    mism = int((fl != g["flags"]).sum())
+    assert mism <= max(2, g["flags"].size // 10000), f"{mism} flags differ"
+
+
+@pytest.mark.gpu
+def test_dose_c1_matches_reference(ctx):
+    """Config 1, all 100 beamlets through the library's own Terma, CCCS and
+    column stages; the summed dose against the reference's summed columns."""
+    g = _gold("dose_c1_ref.npz")
+    case = c1_case()
+    dens = api.Density(ctx, case["phantom"].density, case["phantom"].volume)
+    m = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, api.Spectrum(ctx, case["cfg"]["spectrum"]),
+                                api.Kernel(ctx, _c1_kernel(g)))
+    ro, col, val = m.to_host()
+    nnz = np.diff(ro)
+    dose = np.zeros(g["dose_sum"].size, np.float64)
+    np.add.at(dose, col, val)
+    _gate(dose, g["dose_sum"].ravel())
+    # row supports agree up to the point-sampling flips at the column edges
+    assert np.abs(nnz - g["nnz"]).max() <= 0.02 * g["nnz"].max()
