@@ -48,6 +48,9 @@ _PROTOS = {
     "fd2_csr_ensemble_destroy": (_i, [_vp]),
     "fd2_beamlet_flags_save": (_i, [_vp, _sz, C.c_char_p]),
     "fd2_cccs_cone_directions": (_i, [_vp, _vp, _sz, _vp, _vp, _sz]),
+    "fd2_context_set_timing": (_i, [_vp, _i]),
+    "fd2_context_stage_times": (_i, [_vp, _vp, _i]),
+    "fd2_context_launch_count": (C.c_uint64, [_vp]),
     "fd2_bev2pvcs_interp": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 

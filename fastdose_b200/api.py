@@ -79,6 +79,20 @@ class Context:
     def synchronize(self):
         _lib.check(self.lib.fd2_context_synchronize(self.h), "context_synchronize")
 
+    STAGES = ("terma", "cccs", "columns", "opt_spmv", "opt_other")
+
+    def set_timing(self, on=True):
+        _lib.check(self.lib.fd2_context_set_timing(self.h, int(on)), "set_timing")
+
+    def stage_times(self):
+        """Accumulated device ms per stage since the last call (then reset)."""
+        out = np.zeros(len(self.STAGES), np.float64)
+        _lib.check(self.lib.fd2_context_stage_times(self.h, _p(out), len(out)), "stage_times")
+        return dict(zip(self.STAGES, out.tolist()))
+
+    def launch_count(self):
+        return int(self.lib.fd2_context_launch_count(self.h))
+
     def close(self):
         if self.h:
             self.lib.fd2_context_destroy(self.h)

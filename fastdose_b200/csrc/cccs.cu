@@ -84,10 +84,25 @@ __device__ __forceinline__ bool crosses_edge(float b, float n, float ff) {
     return floorf(__fdividef(b, ff)) != floorf(__fdividef(n, ff));
 }
 
+// The same two operations for a 16-pixel map axis.  Division by 16 is exact
+// (the fast reciprocal of a power of two is exact), so b / 16 is b * 0.0625; the
+// remainder m - 16*trunc(m/16) is exact by Sterbenz's lemma and equals fmodf.
+__device__ __forceinline__ int mid_index16(float b, float n) {
+    const float m = __fmul_rn(__fadd_rn(b, n), 0.5f);
+    float r = __fsub_rn(m, __fmul_rn(16.0f, truncf(__fmul_rn(m, 0.0625f))));
+    r = r < 0.0f ? __fadd_rn(r, 16.0f) : r;
+    const int i = __float2int_rd(r);
+    return i < 16 ? i : 15;
+}
+
+__device__ __forceinline__ bool crosses16(float b, float n) {
+    return floorf(__fmul_rn(b, 0.0625f)) != floorf(__fmul_rn(n, 0.0625f));
+}
+
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
 // the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
-// sums).  RPL = rays per lane (P <= 32 * RPL).
-template <int RPL>
+// sums).  RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
+template <int RPL, bool kFx16>
 __global__ void __launch_bounds__(768) cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
@@ -171,6 +186,36 @@ __global__ void __launch_bounds__(768) cccs_kernel(const fd2_beam_t* __restrict_
                 const float fe = (np.z * g.ls + g.lim_min) * g.inv_sad;
                 const float fs = (c.z * g.ls + g.lim_min) * g.inv_sad;
                 const float dzp = (np.z - c.z) * g.ls;
+                if constexpr (kFx16) {
+                    // 16x16 map: a lane's rays share their column, so the x half of
+                    // the voxel/edge/length work is done once per lane per step
+                    const float lx = (float)(lane & 15);
+                    const float btx = __fadd_rn(c.x, lx), ntx = __fadd_rn(np.x, lx);
+                    const int cx = mid_index16(btx, ntx);
+                    const bool wrapx = crosses16(btx, ntx);
+                    const float dxp = (ntx - 8.0f) * g.bsx * fe - (btx - 8.0f) * g.bsx * fs;
+                    const float dxz2 = dxp * dxp + dzp * dzp;
+#pragma unroll
+                    for (int j = 0; j < RPL; j++) {
+                        const float ly = (float)((lane >> 4) + 2 * j);
+                        const float bty = __fadd_rn(c.y, ly), nty = __fadd_rn(np.y, ly);
+                        const int mi = cx + 16 * mid_index16(bty, nty);
+                        const bool wrap = wrapx || crosses16(bty, nty);
+                        const float dyp = (nty - 8.0f) * g.bsy * fe - (bty - 8.0f) * g.bsy * fs;
+                        const float l2 = dxz2 + dyp * dyp;
+                        const float len = l2 * rsqrtf(l2);
+                        const float2 trv = tr[mi];
+                        const float p = len * trv.y;
+                        const float ea = __expf(-ka * p), eb = __expf(-kb * p);
+                        const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
+                        float2 acc = mydp[mi];
+                        acc.x += dep;
+                        acc.y += p;
+                        mydp[mi] = acc;
+                        XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
+                        XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
+                    }
+                } else {
 #pragma unroll
                 for (int j = 0; j < RPL; j++) {
                     const float btx = __fadd_rn(c.x, fix[j]), ntx = __fadd_rn(np.x, fix[j]);
@@ -196,6 +241,7 @@ __global__ void __launch_bounds__(768) cccs_kernel(const fd2_beam_t* __restrict_
                     }
                     XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                     XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
+                }
                 }
                 c = np;
                 __syncwarp();
@@ -296,20 +342,31 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     const int threads = 32 * k->n_phi;
     const size_t shm = (size_t)(1 + k->n_phi) * maxP * sizeof(float2);
     const unsigned blocks = (unsigned)(schedule == 1 ? n_beams * fwd.size() : n_beams);
-    if (maxP <= 256) {
-        FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<8><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
-                                                         d_planes, plane_stride, ctx->d_status);
+    bool all16 = true;
+    for (size_t i = 0; i < n_beams && all16; i++) all16 = h_beams[i].fmap_size[0] == 16 && h_beams[i].fmap_size[1] == 16;
+    if (all16) {
+        FD2_CHECK_CUDA(
+            cudaFuncSetAttribute(cccs_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<8, true><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
+                                                               d_planes, plane_stride, ctx->d_status);
+    } else if (maxP <= 256) {
+        FD2_CHECK_CUDA(
+            cudaFuncSetAttribute(cccs_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<8, false><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp,
+                                                                schedule, d_planes, plane_stride, ctx->d_status);
     } else {
-        FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<32><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
-                                                          d_planes, plane_stride, ctx->d_status);
+        FD2_CHECK_CUDA(
+            cudaFuncSetAttribute(cccs_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<32, false><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp,
+                                                                 schedule, d_planes, plane_stride, ctx->d_status);
     }
     FD2_CHECK_CUDA(cudaGetLastError());
+    ctx->launches += 2;  // direction table + march
     if (schedule == 1) {
         dim3 grid(std::max(1, std::min(64, (int)((plane_stride + 255) / 256))), (unsigned)n_beams);
         cccs_split_reduce<<<grid, 256, 0, stream>>>(d_beams, d_dose, d_planes, plane_stride, (int)fwd.size());
         FD2_CHECK_CUDA(cudaGetLastError());
+        ctx->launches += 1;
     }
     return FD2_OK;
 }

@@ -66,6 +66,21 @@ int fd2_context_synchronize(fd2_context* c) {
     return FD2_OK;
 }
 
+int fd2_context_set_timing(fd2_context* c, int on) {
+    FD2_REQUIRE(c, FD2_ERR_INVALID_ARGUMENT, "null context");
+    c->timing = on ? 1 : 0;
+    return FD2_OK;
+}
+
+int fd2_context_stage_times(fd2_context* c, double* ms, int n) {
+    FD2_REQUIRE(c && ms, FD2_ERR_INVALID_ARGUMENT, "null argument");
+    for (int i = 0; i < n && i < FD2_STAGE_COUNT; i++) ms[i] = c->stage_ms[i];
+    for (int i = 0; i < FD2_STAGE_COUNT; i++) c->stage_ms[i] = 0.0;
+    return FD2_OK;
+}
+
+uint64_t fd2_context_launch_count(const fd2_context* c) { return c ? c->launches : 0; }
+
 int fd2_density_create(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume, fd2_density** out) {
     FD2_REQUIRE(ctx && host_density && volume && out, FD2_ERR_INVALID_ARGUMENT, "density_create: null argument");
     size_t nv = (size_t)volume->dim[0] * volume->dim[1] * volume->dim[2];

@@ -215,6 +215,7 @@ static int append_columns(fd2_csr_ensemble* e, const fd2_beam_t* hb, size_t nb, 
         FD2_CHECK_CUDA(cudaStreamSynchronize(st));
         e->n_rows += nb;
         e->nnz = (uint64_t)roff[nb];
+        e->ctx->launches += 3;  // count, values, gather
         return FD2_OK;
     }();
     for (void* p : {(void*)d_infos, (void*)d_cnt, (void*)d_nnz, (void*)d_cap_off, (void*)d_roff, (void*)d_tcol,
@@ -355,12 +356,23 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
             FD2_TRY(upload(hR, &aR, st));
             FD2_TRY(upload(hD, &aD, st));
             FD2_CHECK_CUDA(cudaMemsetAsync(dD, 0, off[nb] * sizeof(float), st));
-            FD2_TRY(launch_terma(ctx, P, nb, d_beams + b0, aF, aT, aR, density, spectrum, 1, st));
-            int sched = params.cccs_schedule >= 0 ? params.cccs_schedule : cccs_auto_schedule(ctx, nb);
-            FD2_TRY(launch_cccs_host(ctx, nb, beams.data() + b0, d_beams + b0, (const float* const*)aT,
-                                     (const float* const*)aR, aD, kernel, sched, st));
-            return append_columns(e, beams.data() + b0, nb, (const float* const*)aD, vol, params.extent,
-                                  params.ss_factor, st);
+            {
+                StageTimer t(ctx, st, FD2_STAGE_TERMA);
+                FD2_TRY(launch_terma(ctx, P, nb, d_beams + b0, aF, aT, aR, density, spectrum, 1, st));
+                t.stop();
+            }
+            {
+                StageTimer t(ctx, st, FD2_STAGE_CCCS);
+                int sched = params.cccs_schedule >= 0 ? params.cccs_schedule : cccs_auto_schedule(ctx, nb);
+                FD2_TRY(launch_cccs_host(ctx, nb, beams.data() + b0, d_beams + b0, (const float* const*)aT,
+                                         (const float* const*)aR, aD, kernel, sched, st));
+                t.stop();
+            }
+            StageTimer t(ctx, st, FD2_STAGE_COLUMNS);
+            int r = append_columns(e, beams.data() + b0, nb, (const float* const*)aD, vol, params.extent,
+                                   params.ss_factor, st);
+            t.stop();
+            return r;
         }();
         // release batch buffers
         for (void* p : {(void*)d_bev, (void*)aF, (void*)aT, (void*)aR, (void*)aD})

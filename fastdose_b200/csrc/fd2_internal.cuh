@@ -63,7 +63,41 @@ struct fd2_context {
     // reusable scratch, grown on demand
     void* scratch = nullptr;
     size_t scratch_bytes = 0;
+    // instrumentation: kernels launched, and (when enabled) device time per stage
+    uint64_t launches = 0;
+    int timing = 0;
+    double stage_ms[FD2_STAGE_COUNT] = {0};
 };
+
+namespace fd2 {
+// Brackets one stage of work on a stream with CUDA events when the context's
+// timing is on; the elapsed time is added to ctx->stage_ms[stage] at finish().
+struct StageTimer {
+    fd2_context* ctx;
+    cudaStream_t st;
+    int stage;
+    cudaEvent_t a = nullptr, b = nullptr;
+    StageTimer(fd2_context* c, cudaStream_t s, int stg) : ctx(c), st(s), stage(stg) {
+        if (ctx->timing) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, st);
+        }
+    }
+    void stop() {
+        if (ctx->timing && b) cudaEventRecord(b, st);
+    }
+    ~StageTimer() {
+        if (ctx->timing && a && b) {
+            float ms = 0.0f;
+            if (cudaEventSynchronize(b) == cudaSuccess && cudaEventElapsedTime(&ms, a, b) == cudaSuccess)
+                ctx->stage_ms[stage] += ms;
+        }
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+};
+}  // namespace fd2
 
 struct fd2_density {
     fd2_context* ctx = nullptr;

@@ -101,24 +101,46 @@ __device__ __forceinline__ bool candidate(const ColumnInfo& ci, float3 c, float 
 }
 
 // Mean of ss^3 point samples (d_voxelInterp), or 0 when the voxel centre is
-// farther than extent + hdiag from the beamlet axis.
+// farther than extent + hdiag from the beamlet axis.  Sample positions are
+// affine in the sub-sample indices, so the beam-frame coordinates are stepped
+// incrementally; one reciprocal of the depth per sample gives the divergent
+// lateral scale; consecutive samples that land in the same texel reuse it.
 __device__ __forceinline__ float column_value(const ColumnInfo& ci, const float* __restrict__ bev, int x, int y,
                                               int z, float3 vs, float hdiag, float extent, int ss) {
-    float3 c = make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z);
-    float3 v = rot(ci.R, make_float3(c.x - ci.src[0], c.y - ci.src[1], c.z - ci.src[2]));
+    const float3 c = make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z);
+    const float3 v = rot(ci.R, make_float3(c.x - ci.src[0], c.y - ci.src[1], c.z - ci.src[2]));
     if (sqrtf(v.x * v.x + v.z * v.z) > hdiag + extent) return 0.0f;
     const float inv = 1.0f / ss;
     const float ffx = (float)ci.fx, ffy = (float)ci.fy;
-    float acc = 0.0f;
+    const float a = inv * vs.x, b = inv * vs.y, cz = inv * vs.z;
+    const float3 dI = make_float3(ci.R[0] * a, ci.R[3] * a, ci.R[6] * a);
+    const float3 dJ = make_float3(ci.R[1] * b, ci.R[4] * b, ci.R[7] * b);
+    const float3 dK = make_float3(ci.R[2] * cz, ci.R[5] * cz, ci.R[8] * cz);
+    const float3 p0 = make_float3((x + 0.5f * inv) * vs.x - ci.src[0], (y + 0.5f * inv) * vs.y - ci.src[1],
+                                  (z + 0.5f * inv) * vs.z - ci.src[2]);
+    const float3 u0 = rot(ci.R, p0);
+    const float sx = 1.0f / (ci.bsx * ci.inv_sad), sz = 1.0f / (ci.bsy * ci.inv_sad);
+    const int plane = ci.fx * ci.fy;
+    int last = -1;
+    float last_v = 0.0f, acc = 0.0f;
     for (int kk = 0; kk < ss; kk++) {
-        const float pz = (z + (kk + 0.5f) * inv) * vs.z;
+        const float3 uk = make_float3(u0.x + kk * dK.x, u0.y + kk * dK.y, u0.z + kk * dK.z);
         for (int jj = 0; jj < ss; jj++) {
-            const float py = (y + (jj + 0.5f) * inv) * vs.y;
+            const float3 ukj = make_float3(uk.x + jj * dJ.x, uk.y + jj * dJ.y, uk.z + jj * dJ.z);
             for (int ii = 0; ii < ss; ii++) {
-                const float px = (x + (ii + 0.5f) * inv) * vs.x;
-                float3 cn = to_bev_grid(ci, make_float3(px, py, pz));
-                if (cn.x < 0.0f || cn.x > ffx || cn.z < 0.0f || cn.z > ffy) continue;
-                acc += bev_fetch(bev, ci.fx, ci.fy, ci.L, (int)floorf(cn.x), (int)floorf(cn.z), (int)floorf(cn.y));
+                const float ux = ukj.x + ii * dI.x, uy = ukj.y + ii * dI.y, uz = ukj.z + ii * dI.z;
+                const float r = __fdividef(1.0f, uy);
+                const float cnx = ux * r * sx + ci.hx, cnz = uz * r * sz + ci.hy;
+                if (cnx < 0.0f || cnx > ffx || cnz < 0.0f || cnz > ffy) continue;
+                const int tx = __float2int_rd(cnx), ty = __float2int_rd(cnz);
+                const int tz = __float2int_rd((uy - ci.lim_min) * ci.inv_ls);
+                if (tx >= ci.fx || ty >= ci.fy || (unsigned)tz >= (unsigned)ci.L) continue;
+                const int idx = tx + ci.fx * ty + plane * tz;
+                if (idx != last) {
+                    last = idx;
+                    last_v = __ldg(bev + idx);
+                }
+                acc += last_v;
             }
         }
     }
@@ -126,6 +148,8 @@ __device__ __forceinline__ float column_value(const ColumnInfo& ci, const float*
 }
 
 constexpr int kColThreads = 256;
+constexpr int kPerThread = 4;
+constexpr int kColChunk = kColThreads * kPerThread;
 
 // Pass 1: number of candidate voxels of each beamlet (its row capacity).
 __global__ void __launch_bounds__(kColThreads) column_count_kernel(const ColumnInfo* __restrict__ infos,
@@ -162,28 +186,66 @@ __global__ void __launch_bounds__(kColThreads) column_value_kernel(
     typedef cub::BlockReduce<float, kColThreads> RMax;
     __shared__ typename Scan::TempStorage scan_tmp;
     __shared__ typename RMax::TempStorage max_tmp;
+    __shared__ int s_cand[kColChunk];    // box-relative indices of this chunk's candidates, in order
+    __shared__ float s_val[kColChunk];
     uint32_t written = 0;  // uniform across the block
     float vmax = 0.0f;
-    for (long long i0 = 0; i0 < n; i0 += kColThreads) {
-        long long i = i0 + threadIdx.x;
-        float val = 0.0f;
-        int32_t col = 0;
-        if (i < n) {
-            int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by),
-                z = ci.box[2] + (int)(i / ((long long)bx * by));
-            col = x + nx * (y + ny * z);
-            if (candidate(ci, make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z), hdiag, extent))
-                val = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
+    const long long bxy = (long long)bx * by;
+    for (long long i0 = 0; i0 < n; i0 += kColChunk) {
+        // 1. candidate test, kPerThread consecutive voxels per thread (order-preserving compaction)
+        uint32_t flags = 0, cnt = 0;
+#pragma unroll
+        for (int q = 0; q < kPerThread; q++) {
+            const long long i = i0 + (long long)threadIdx.x * kPerThread + q;
+            if (i < n) {
+                const int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by),
+                          z = ci.box[2] + (int)(i / bxy);
+                if (candidate(ci, make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z), hdiag,
+                              extent)) {
+                    flags |= 1u << q;
+                    cnt++;
+                }
+            }
         }
-        uint32_t nz = val != 0.0f, pos, total;
-        Scan(scan_tmp).ExclusiveSum(nz, pos, total);
-        if (nz && written + pos < cap) {
-            tmp_col[base + written + pos] = col;
-            tmp_val[base + written + pos] = val;
+        uint32_t pos, n_cand;
+        Scan(scan_tmp).ExclusiveSum(cnt, pos, n_cand);
+#pragma unroll
+        for (int q = 0; q < kPerThread; q++)
+            if (flags & (1u << q)) s_cand[pos++] = (int)(threadIdx.x * kPerThread + q);
+        __syncthreads();
+        // 2. values of the candidates, spread over all threads
+        for (uint32_t k = threadIdx.x; k < n_cand; k += kColThreads) {
+            const long long i = i0 + s_cand[k];
+            const int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by), z = ci.box[2] + (int)(i / bxy);
+            s_val[k] = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
         }
-        vmax = fmaxf(vmax, fabsf(val));
-        written += total;
-        __syncthreads();  // scan_tmp reuse
+        __syncthreads();
+        // 3. nonzeros in order into the row's segment
+        uint32_t nzc = 0;
+#pragma unroll
+        for (int q = 0; q < kPerThread; q++) {
+            const uint32_t k = threadIdx.x * kPerThread + q;
+            if (k < n_cand && s_val[k] != 0.0f) nzc++;
+        }
+        uint32_t npos, n_nz;
+        Scan(scan_tmp).ExclusiveSum(nzc, npos, n_nz);
+#pragma unroll
+        for (int q = 0; q < kPerThread; q++) {
+            const uint32_t k = threadIdx.x * kPerThread + q;
+            if (k < n_cand && s_val[k] != 0.0f) {
+                const long long i = i0 + s_cand[k];
+                const int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by),
+                          z = ci.box[2] + (int)(i / bxy);
+                if (written + npos < cap) {
+                    tmp_col[base + written + npos] = x + nx * (y + ny * z);
+                    tmp_val[base + written + npos] = s_val[k];
+                }
+                vmax = fmaxf(vmax, fabsf(s_val[k]));
+                npos++;
+            }
+        }
+        written += n_nz;
+        __syncthreads();  // s_cand / s_val / scan_tmp reuse
     }
     float m = RMax(max_tmp).Reduce(vmax, cub::Max());
     if (threadIdx.x == 0) {

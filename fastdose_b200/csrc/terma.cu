@@ -136,6 +136,7 @@ int launch_terma(fd2_context* ctx, size_t fmap_npixels, size_t n_beams, const fd
                                                         v.dim[0], v.dim[1], v.dim[2], v.voxel_size[0],
                                                         v.voxel_size[1], v.voxel_size[2], sp);
     FD2_CHECK_CUDA(cudaGetLastError());
+    if (ctx) ctx->launches += 1;
     return FD2_OK;
 }
 

@@ -130,6 +130,26 @@ int fd2_context_destroy(fd2_context* ctx);
 int fd2_context_synchronize(fd2_context* ctx);
 
 /*
+ * Instrumentation, the counterpart of the reference's per-kernel event timers
+ * (FastDoseLib/src/TermaComp.cu:311-333, DoseComp.cu:450-472,
+ * IMRTOpt/src/IMRTDoseMat.cu:261-274).  With timing on, the plan-level calls
+ * bracket each stage with CUDA events and accumulate its device time.
+ */
+enum fd2_stage {
+    FD2_STAGE_TERMA = 0,
+    FD2_STAGE_CCCS = 1,
+    FD2_STAGE_COLUMNS = 2,
+    FD2_STAGE_OPT_SPMV = 3,
+    FD2_STAGE_OPT_OTHER = 4,
+    FD2_STAGE_COUNT = 5
+};
+int fd2_context_set_timing(fd2_context* ctx, int on);
+/* Copies min(n, FD2_STAGE_COUNT) accumulated stage times (ms) and resets them. */
+int fd2_context_stage_times(fd2_context* ctx, double* ms, int n);
+/* Number of kernels this library launched through the context so far. */
+uint64_t fd2_context_launch_count(const fd2_context* ctx);
+
+/*
  * fastdose::density_h2d (FastDoseLib/src/density.cu:23-58).  Copies a host
  * density volume to the device.  Sampling is trilinear on texel centres i+0.5
  * with zero outside the volume (the reference's linear/border texture).
