@@ -52,6 +52,7 @@ _PROTOS = {
     "fd2_context_stage_times": (_i, [_vp, _vp, _i]),
     "fd2_context_launch_count": (C.c_uint64, [_vp]),
     "fd2_bev2pvcs_interp": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "fd2_dose_compute_static": (_i, [_sz, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _LIB = None

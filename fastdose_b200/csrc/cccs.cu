@@ -30,6 +30,8 @@
 // the identical operations, so both march the same segments bit for bit.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "fd2_internal.cuh"
@@ -421,5 +423,151 @@ extern "C" int fd2_cccs_cone_directions(fd2_context* ctx, const fd2_cccs_kernel*
     if (d_out) cudaFree(d_out);
     if (rc) return rc;
     FD2_CHECK_CUDA(e);
+    return FD2_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fd2_dose_compute_static: the CCCS march without any device allocation.
+//
+// fd2_dose_compute keeps its cone-direction table (and, for batches too small
+// to fill the device, per-zenith planes) in the context's scratch buffer,
+// which grows with cudaMalloc when a larger batch arrives.  Some hosts cannot
+// allow that: a treatment-planning service that hands out every byte of device
+// memory from its own pool sized at start-up, or a caller whose device memory
+// is owned by another runtime that forbids foreign allocations once its pools
+// are set.  Those callers get this entry point: no context, no cudaMalloc, no
+// cudaFree, no allocating library.  What it needs beyond the caller's buffers
+// -- the status word and the direction table -- lives in one fixed array in
+// device global memory, defined below; its address is looked up once per
+// device with cudaGetSymbolAddress on the first call.
+//
+// Limits: n_beams * n_forward_theta * n_phi * 16 bytes of directions must fit
+// FD2_DOSE_STATIC_DIR_BYTES (256 KiB: 256 beams of an 8 x 8 cone kernel);
+// larger batches are rejected with FD2_ERR_CAPACITY before any device work.
+// Only schedule 0 runs (every zenith bin of a beamlet in one block, no
+// planes), whose dose equals schedule 1's bit for bit.
+//
+// Every call shares the one array on its device: two calls whose work
+// overlaps on the device (different streams, or different host threads with
+// no ordering between them) overwrite each other's direction table and status
+// word.  Serialise them (same stream, or synchronise in between).
+
+// [0, 256): status word, cleared by every call before its launches (the only
+// part that must start at zero); [256, 256 + FD2_DOSE_STATIC_DIR_BYTES):
+// direction table [beam][theta_fwd][phi] as float4, fully rewritten by every call.
+static __device__ __align__(256) unsigned char fd2_static_scratch[256 + FD2_DOSE_STATIC_DIR_BYTES];
+
+namespace {
+
+constexpr size_t kStaticStatusBytes = 256;  // fd2::DeviceStatus, padded to keep the table aligned
+constexpr size_t kStaticDirBytes = FD2_DOSE_STATIC_DIR_BYTES;
+constexpr int kStaticMaxDevices = 64;
+constexpr size_t kBeamChunk = 32;  // beam descriptors read back per copy, on the host stack
+static_assert(sizeof(fd2::DeviceStatus) <= kStaticStatusBytes, "status word outgrew its slot");
+
+void* g_static_addr[kStaticMaxDevices];
+std::mutex g_static_mu;
+
+// The device address of fd2_static_scratch on the current device.  Host code
+// only sees a stand-in for the array's name, so the address is looked up with
+// cudaGetSymbolAddress, once per device, and cached.
+int static_scratch_address(unsigned char** out) {
+    int dev = 0;
+    FD2_CHECK_CUDA(cudaGetDevice(&dev));
+    FD2_REQUIRE(dev >= 0 && dev < kStaticMaxDevices, FD2_ERR_NOT_SUPPORTED,
+                "dose_compute_static: device ordinal %d beyond %d", dev, kStaticMaxDevices);
+    std::lock_guard<std::mutex> lock(g_static_mu);
+    if (!g_static_addr[dev]) {
+        void* p = nullptr;
+        FD2_CHECK_CUDA(cudaGetSymbolAddress(&p, fd2_static_scratch));
+        FD2_REQUIRE(p != nullptr && ((uintptr_t)p & 255) == 0, FD2_ERR_CUDA,
+                    "dose_compute_static: scratch address %p not 256-byte aligned", p);
+        g_static_addr[dev] = p;
+    }
+    *out = (unsigned char*)g_static_addr[dev];
+    return FD2_OK;
+}
+
+}  // namespace
+
+extern "C" int fd2_dose_compute_static(size_t fmap_npixels, size_t n_beams, const fd2_beam_t* d_beams,
+                                       float* const* d_terma, float* const* d_density_bev, float* const* d_dose,
+                                       const fd2_cccs_kernel* kernel, int* status_out, void* stream) {
+    using namespace fd2;
+    FD2_REQUIRE(d_beams && d_terma && d_density_bev && d_dose && kernel, FD2_ERR_INVALID_ARGUMENT,
+                "dose_compute_static: null argument");
+    FD2_REQUIRE(fmap_npixels > 0 && fmap_npixels <= 1024, FD2_ERR_INVALID_ARGUMENT,
+                "dose_compute_static: fmap_npixels %zu outside 1..1024", fmap_npixels);
+    if (n_beams == 0) return FD2_OK;
+    const fd2_cccs_kernel* k = kernel;
+    ConeParams cp{};
+    ConeAngles ang{};
+    for (int t = 0; t < k->n_theta; t++) {
+        if ((double)k->theta[t] > 1.5707963267948966) continue;  // forward bins only, DoseComp.cu:265
+        const int i = cp.n_theta_fwd++;
+        cp.a[i] = k->a[t];
+        cp.b[i] = k->b[t];
+        cp.A_a[i] = k->A[t] / k->a[t];
+        cp.B_b[i] = k->B[t] / k->b[t];
+        ang.theta[i] = k->theta[t];
+    }
+    if (cp.n_theta_fwd == 0) return FD2_OK;
+    cp.n_phi = ang.n_phi = k->n_phi;
+    ang.n_theta_fwd = cp.n_theta_fwd;
+    for (int f = 0; f < k->n_phi; f++) ang.phi[f] = k->phi[f];
+    const size_t per_beam = (size_t)cp.n_theta_fwd * cp.n_phi * sizeof(float4);
+    FD2_REQUIRE(n_beams <= kStaticDirBytes / per_beam, FD2_ERR_CAPACITY,
+                "dose_compute_static: %zu beams x %d cones need %zu bytes of direction table; the fixed scratch "
+                "holds %zu bytes (at most %zu beams of this kernel per call)",
+                n_beams, cp.n_theta_fwd * cp.n_phi, n_beams * per_beam, kStaticDirBytes, kStaticDirBytes / per_beam);
+
+    // map sizes of the batch, read back in chunks through a small stack buffer
+    cudaStream_t st = (cudaStream_t)stream;
+    fd2_beam_t hb[kBeamChunk];
+    int maxP = 0;
+    bool all16 = true;
+    for (size_t i0 = 0; i0 < n_beams; i0 += kBeamChunk) {
+        const size_t m = std::min(kBeamChunk, n_beams - i0);
+        FD2_CHECK_CUDA(cudaMemcpyAsync(hb, d_beams + i0, m * sizeof(fd2_beam_t), cudaMemcpyDeviceToHost, st));
+        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+        for (size_t i = 0; i < m; i++) {
+            FD2_REQUIRE(hb[i].TermaBEV_pitch == hb[i].DensityBEV_pitch, FD2_ERR_INVALID_ARGUMENT,
+                        "dose_compute_static: Terma and density pitches differ");
+            maxP = std::max(maxP, (int)(hb[i].fmap_size[0] * hb[i].fmap_size[1]));
+            all16 = all16 && hb[i].fmap_size[0] == 16 && hb[i].fmap_size[1] == 16;
+        }
+    }
+    FD2_REQUIRE(maxP > 0 && maxP <= 1024, FD2_ERR_INVALID_ARGUMENT,
+                "dose_compute_static: fmap of %d pixels (1..1024)", maxP);
+
+    unsigned char* base = nullptr;
+    FD2_TRY(static_scratch_address(&base));
+    DeviceStatus* d_status = (DeviceStatus*)base;
+    float4* d_dirs = (float4*)(base + kStaticStatusBytes);
+    FD2_CHECK_CUDA(cudaMemsetAsync(d_status, 0, sizeof(DeviceStatus), st));
+    FD2_TRY(launch_cone_dirs(d_beams, n_beams, ang, d_dirs, st));
+    const int threads = 32 * cp.n_phi;
+    const size_t shm = (size_t)(1 + cp.n_phi) * maxP * sizeof(float2);
+    const unsigned blocks = (unsigned)n_beams;
+    const float* const* T = (const float* const*)d_terma;
+    const float* const* R = (const float* const*)d_density_bev;
+    if (all16) {
+        FD2_CHECK_CUDA(
+            cudaFuncSetAttribute(cccs_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<8, true><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0, d_status);
+    } else if (maxP <= 256) {
+        FD2_CHECK_CUDA(
+            cudaFuncSetAttribute(cccs_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<8, false><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0,
+                                                            d_status);
+    } else {
+        FD2_CHECK_CUDA(
+            cudaFuncSetAttribute(cccs_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
+        cccs_kernel<32, false><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0,
+                                                             d_status);
+    }
+    FD2_CHECK_CUDA(cudaGetLastError());
+    if (status_out)
+        FD2_CHECK_CUDA(cudaMemcpyAsync(status_out, &d_status->code, sizeof(int), cudaMemcpyDefault, st));
     return FD2_OK;
 }

@@ -201,6 +201,42 @@ int fd2_dose_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_beams,
                      float* const* d_density_bev, float* const* d_dose,
                      const fd2_cccs_kernel* kernel, void* stream);
 
+/* Direction-table capacity of fd2_dose_compute_static, in bytes. */
+#define FD2_DOSE_STATIC_DIR_BYTES (256u * 1024u)
+
+/*
+ * fd2_dose_compute without any device allocation.  No counterpart in the
+ * reference: an addition for callers that may not allocate device memory
+ * while they run (their device memory is carved from a pool fixed at
+ * start-up, or owned by another runtime that forbids foreign allocations).
+ * Same arguments and result as fd2_dose_compute, without a context: the
+ * status word and the cone-direction table live in one fixed array in device
+ * global memory (FD2_DOSE_STATIC_DIR_BYTES + 256 bytes, held by every GPU that
+ * loads the library until exit), and nothing is allocated by cudaMalloc or
+ * any library.
+ *
+ * - The first call on each device looks up that array's address (which may
+ *   load the library's device code onto the device); make it during set-up,
+ *   before any stream capture.
+ * - Limit: n_beams * n_forward_theta * n_phi * 16 <= FD2_DOSE_STATIC_DIR_BYTES
+ *   (256 beams of an 8 x 8 cone kernel); larger batches return
+ *   FD2_ERR_CAPACITY before any device work.
+ * - Accumulates (+=) into d_dose like fd2_dose_compute: zero it first for a
+ *   fresh dose.  The call clears its own status word; nothing else in the
+ *   fixed array needs to start at zero.
+ * - status_out (NULL, host or device int): receives the kernels' status code
+ *   (0, or FD2_ERR_WATCHDOG) in stream order; read it after the stream
+ *   synchronises.
+ * - All calls on one device share the fixed array: calls whose device work
+ *   overlaps (different streams, or unordered host threads) race and corrupt
+ *   each other.  Serialise them.
+ * The beam descriptors are read back to the host (synchronising the stream)
+ * to size the launch.
+ */
+int fd2_dose_compute_static(size_t fmap_npixels, size_t n_beams, const fd2_beam_t* d_beams,
+                            float* const* d_terma, float* const* d_density_bev, float* const* d_dose,
+                            const fd2_cccs_kernel* kernel, int* status_out, void* stream);
+
 /*
  * The cone directions the CCCS march uses: for every beam, forward zenith bin
  * (theta <= pi/2) and azimuth, the unit direction in normalised BEV units,
