@@ -15,6 +15,7 @@ _i = C.c_int
 _sz = C.c_size_t
 _f = C.c_float
 _u64 = C.c_uint64
+_i64 = C.c_int64
 
 _PROTOS = {
     "fd2_status_string": (C.c_char_p, [_i]),
@@ -53,6 +54,24 @@ _PROTOS = {
     "fd2_context_launch_count": (C.c_uint64, [_vp]),
     "fd2_bev2pvcs_interp": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "fd2_dose_compute_static": (_i, [_sz, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    # optimizer (fd2_opt.h)
+    "fd2_matrix_create": (_i, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _i, _vp]),
+    "fd2_matrix_destroy": (_i, [_vp]),
+    "fd2_matrix_info": (_i, [_vp, _vp]),
+    "fd2_matrix_to_host": (_i, [_vp, _vp, _vp, _vp]),
+    "fd2_matrix_transpose": (_i, [_vp, _vp]),
+    "fd2_matrix_spmv": (_i, [_vp, _vp, _vp, _vp]),
+    "fd2_voi_matrices": (_i, [_vp, _vp, _i64, _i64, _i, _vp, _vp]),
+    "fd2_matrix_synthetic": (_i, [_vp, _i64, _i64, _i64, _f, _u64, _i, _vp, _vp]),
+    "fd2_fluence_grad": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "fd2_opt_problem_create": (_i, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp]),
+    "fd2_opt_problem_destroy": (_i, [_vp]),
+    "fd2_eval_g": (_i, [_vp, _vp, _vp]),
+    "fd2_eval_grad": (_i, [_vp, _vp, _vp, _vp]),
+    "fd2_prox_l2onehalf": (_i, [_vp, _i64, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "fd2_beam_weights_init": (_i, [_vp, _i64, _vp, _vp]),
+    "fd2_boo_l2onehalf": (_i, [_vp, _i64, _vp, _vp, _i, _i, _i, _vp, _i, _i, _vp]),
+    "fd2_polish": (_i, [_vp, _i, _i, _vp]),
 }
 
 _LIB = None

@@ -640,3 +640,7 @@ int fd2_beamlet_flags_save(const uint8_t* flags, size_t n, const char* path) {
 }
 
 }  // extern "C"
+
+namespace fd2 {
+fd2_context* ensemble_context(const fd2_csr_ensemble* e) { return e->ctx; }
+}  // namespace fd2

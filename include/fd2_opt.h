@@ -1,0 +1,170 @@
+/*
+ * fd2_opt.h -- C ABI of the fluence optimizer: device CSR matrices and their
+ * SpMV, the VOI restriction of a dose-loading matrix, the objective and
+ * gradient of the IMRT problem, the group-sparsity proximal operator and the
+ * two accelerated proximal-gradient solvers.
+ *
+ * Replaces (IMRTOpt, reference layout):
+ *   IMRT::MatCSR64 + Eigen2Cusparse        IMRTOpt/include/IMRTDoseMat.cuh:29-69,
+ *                                          IMRTOpt/src/IMRTEigenLoad.cu:390-435
+ *   getStructFilter + parallelSpGEMM       IMRTOpt/src/IMRTEigenLoad.cu:101-273,
+ *                                          IMRTOpt/src/IMRTEigenLoad.cpp:10-149
+ *   parallelMatCoalesce / transposes       IMRTOpt/src/IMRTEigenLoad.cpp:190-304
+ *   beamWeightsInit_func                   IMRTOpt/src/IMRTOptimize_var1.cu:125-161
+ *   eval_g::evaluate                       IMRTOpt/src/IMRTOptUtils.cu:74-156
+ *   eval_grad::evaluate                    IMRTOpt/src/IMRTOptUtils.cu:512-631
+ *   proxL2Onehalf_QL_gpu::evaluate         IMRTOpt/src/IMRTOptimize_var1.cu:502-570
+ *   BOO_IMRT_L2OneHalf_gpu_QL              IMRTOpt/src/IMRTOptimize.cu:16-194
+ *   polish_BOO_IMRT_gpu                    IMRTOpt/src/IMRTOptimize.cu:391-476
+ *
+ * Matrices hold int64 row offsets, int32 column indices and FP32, FP16 or BF16
+ * values; 16-bit values carry one FP32 scale per column (a matrix of VOI rows x
+ * beamlet columns) or per row (its transpose), so a matrix and its transpose
+ * hold the same rounded values and the gradient stays the exact adjoint of
+ * the objective's product.  Every product accumulates in FP32; the objective
+ * terms, the group norms and the line-search test accumulate in FP64.  All
+ * device pointers are caller-owned unless a handle owns them.
+ */
+#ifndef FD2_OPT_H
+#define FD2_OPT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "fd2.h"
+#include "fd2_imrt.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+#if defined(__GNUC__)
+#pragma GCC visibility push(default)
+#endif
+
+typedef struct fd2_matrix fd2_matrix;
+typedef struct fd2_opt_problem fd2_opt_problem;
+
+typedef enum fd2_scale_axis {
+    FD2_SCALE_NONE = 0,
+    FD2_SCALE_ROWS = 1,
+    FD2_SCALE_COLS = 2
+} fd2_scale_axis;
+
+typedef struct fd2_matrix_info {
+    int64_t rows, cols, nnz;
+    int32_t value_type;   /* fd2_value_type */
+    int32_t scale_axis;   /* fd2_scale_axis */
+    int64_t device_bytes; /* offsets + columns + values + scales */
+} fd2_matrix_info_t;
+
+/*
+ * Upload a host CSR (Eigen2Cusparse): int64 offsets [rows+1], int64 columns
+ * [nnz] (the reference's MatCSR64 index type), FP32 values [nnz].  16-bit
+ * value types are scaled per column (column max -> 1) before rounding.
+ */
+int fd2_matrix_create(fd2_context* ctx, int64_t rows, int64_t cols, int64_t nnz, const int64_t* h_offsets,
+                      const int64_t* h_columns, const float* h_values, int value_type, fd2_matrix** out);
+int fd2_matrix_destroy(fd2_matrix* m);
+int fd2_matrix_info(const fd2_matrix* m, fd2_matrix_info_t* info);
+/* Copy to host as FP32 (scales applied): offsets [rows+1], columns [nnz], values [nnz]. */
+int fd2_matrix_to_host(const fd2_matrix* m, int64_t* h_offsets, int32_t* h_columns, float* h_values);
+/*
+ * Transpose on the device: rows become columns, each new row lists its
+ * columns in ascending order, values move unchanged (a column scale becomes a
+ * row scale and vice versa).
+ */
+int fd2_matrix_transpose(const fd2_matrix* m, fd2_matrix** out);
+/* d_y[rows] = M d_x[cols] (cusparseSpMV with alpha 1, beta 0), FP32 accumulation. */
+int fd2_matrix_spmv(const fd2_matrix* m, const float* d_x, float* d_y, void* stream);
+
+/*
+ * VOI restriction of a dose-loading matrix (getStructFilter + parallelSpGEMM):
+ * h_voxel_row[v] is the VOI row of PVCS voxel v (PTV rows first, then OAR
+ * rows, each structure in voxel order) or -1.  Returns A = [n_voi x beamlets]
+ * and AT = its transpose, in value_type (an FP32 source rounded to 16 bits
+ * with a per-beamlet scale; a 16-bit source keeps its values and scales).
+ * n_voxels must equal the dose matrix's column count.
+ */
+int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, int64_t n_voxels, int64_t n_voi,
+                     int value_type, fd2_matrix** A, fd2_matrix** AT);
+
+/*
+ * Seeded synthetic VOI matrix pair for optimizer benchmarks: rows x cols with
+ * each column j covering a window of `window` consecutive rows centred at
+ * (j + 1/2) rows / cols, each (row, column) of the window kept with
+ * probability `density` (a hash of seed, row and column), the value falling
+ * off with the distance to the window centre.  A and its transpose are
+ * generated independently from the same formula, so they hold identical
+ * values.
+ */
+int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t window, float density, uint64_t seed,
+                         int value_type, fd2_matrix** A, fd2_matrix** AT);
+
+/*
+ * fluenceGradInit for one beam (IMRTOpt/src/IMRTOptimize_var.cpp:59-180 with
+ * DxyInit / KroneckerProduct, IMRTOpt/src/IMRTEigenLoad.cpp:307-407): the CSR
+ * of D_b over the beam's active beamlets (active[fluence_dim^2], row-major
+ * fluence map; beamlet columns numbered in map order), one row (-1, +1) per
+ * pair of horizontally, then vertically, adjacent active pixels.  Caller
+ * capacities: offsets 2 n^2 + 1, columns and values 4 n^2.  Host only.
+ */
+int fd2_fluence_grad(int fluence_dim, const uint8_t* active, int64_t* rows, int64_t* nnz, int64_t* offsets,
+                     int64_t* columns, float* values);
+
+/*
+ * The IMRT problem (eval_g / eval_grad state).  A: [n_ptv + n_oar] x n
+ * (PTV rows first), AT its transpose, D the fluence-gradient rows [m x n],
+ * DT its transpose.  Weight vectors are host arrays: max_dose and
+ * max_weights [n_ptv + n_oar], min_dose and min_weights [n_ptv], oar_weights
+ * [n_oar].  The handle keeps pointers to the four matrices (they must
+ * outlive it) and owns its work vectors.
+ */
+int fd2_opt_problem_create(fd2_context* ctx, const fd2_matrix* A, const fd2_matrix* AT, const fd2_matrix* D,
+                           const fd2_matrix* DT, int64_t n_ptv, int64_t n_oar, const float* h_max_dose,
+                           const float* h_max_weights, const float* h_min_dose, const float* h_min_weights,
+                           const float* h_oar_weights, float gamma, float eta, fd2_opt_problem** out);
+int fd2_opt_problem_destroy(fd2_opt_problem* p);
+
+/* eval_g::evaluate: *h_value = g(d_x) (synchronises the context's stream). */
+int fd2_eval_g(fd2_opt_problem* p, const float* d_x, double* h_value);
+/* eval_grad::evaluate: d_grad[n] = grad g(d_x), *h_value = g(d_x). */
+int fd2_eval_grad(fd2_opt_problem* p, const float* d_x, float* d_grad, double* h_value);
+
+/*
+ * proxL2Onehalf_QL_gpu::evaluate on groups of consecutive entries
+ * (group r = [d_group_offsets[r], d_group_offsets[r+1])): prox of
+ * tau_r * ||x_r||_2^(1/2) at g0, and the new group norms.
+ */
+int fd2_prox_l2onehalf(fd2_context* ctx, int64_t n_groups, const int64_t* d_group_offsets, const float* d_g0,
+                       const float* d_tau, float* d_prox, float* d_nrm, void* stream);
+
+/* beamWeightsInit_func: w_b from the PTV rows of A over each beam's columns. */
+int fd2_beam_weights_init(fd2_opt_problem* p, int64_t n_groups, const int64_t* h_group_offsets, float* h_weights);
+
+/* Solver state carried between calls (the reference's by-reference arguments). */
+typedef struct fd2_opt_state {
+    int32_t k_global;
+    float theta_km1, tkm1;
+    int32_t trials;     /* out: line-search trials in this call */
+    float* d_xkm1;      /* [n] device, in/out */
+    float* d_vkm1;      /* [n] device, in/out */
+    float* h_loss;      /* [iters_global] host, out (may be NULL) */
+    float* h_nrm;       /* [n_groups] host, out (BOO only, may be NULL) */
+    float num_active;   /* out (BOO only) */
+    int32_t stop;       /* out (BOO only) */
+} fd2_opt_state_t;
+
+/* BOO_IMRT_L2OneHalf_gpu_QL (h_beam_weights in/out, h_prune_trigger ascending). */
+int fd2_boo_l2onehalf(fd2_opt_problem* p, int64_t n_groups, const int64_t* h_group_offsets, float* h_beam_weights,
+                      int show_trigger, int change_weights_trigger, int iters_global, const int32_t* h_prune_trigger,
+                      int n_prune, int num_beams_we_want, fd2_opt_state_t* st);
+/* polish_BOO_IMRT_gpu */
+int fd2_polish(fd2_opt_problem* p, int iters_global, int iters_local, fd2_opt_state_t* st);
+
+#if defined(__GNUC__)
+#pragma GCC visibility pop
+#endif
+#ifdef __cplusplus
+}
+#endif
+#endif
