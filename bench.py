@@ -195,6 +195,95 @@ class _DevView:
                                          "strides": None}
 
 
+def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
+    """Fluence optimization on the IMRT-scale synthetic matrix: 2.5M VOI rows
+    (PTV first) x 40k beamlets (400 beams x 10x10 maps), ~2% nonzeros, D from
+    the 10x10 fluence maps, weights as the optimization benchmark states.
+    BOO iterations/s with the matrix in FP32 and in FP16/BF16 (per-beamlet
+    scale), the objective reached by each after the same iterations, and the
+    SpMV bandwidth against the HBM roofline."""
+    import torch
+
+    from fastdose_b200 import optimize
+
+    fd = 10
+    cols = n_beams * fd * fd
+    window, density = rows // 25, 0.5  # each VOI row meets 2% of the beamlets
+    n_ptv = rows // 10
+    rng = np.random.default_rng(seed)
+    n_oar = rows - n_ptv
+    w = dict(max_dose=np.concatenate([np.ones(n_ptv), rng.uniform(0.3, 0.7, n_oar)]).astype(np.float32),
+             max_weights=np.concatenate([np.ones(n_ptv), rng.uniform(0.1, 1.0, n_oar)]).astype(np.float32),
+             min_dose=np.ones(n_ptv, np.float32), min_weights=np.ones(n_ptv, np.float32),
+             oar_weights=rng.uniform(0.0, 0.1, n_oar).astype(np.float32))
+    D = optimize.block_diag([optimize.fluence_grad(fd, np.ones(fd * fd, np.uint8))] * n_beams)
+    Dm = optimize.Matrix.from_csr(ctx, *D[:3], cols)
+    DTm = Dm.transpose()
+    groups = np.arange(0, cols + 1, fd * fd, dtype=np.int64)
+    peak, _ = _peaks()
+    out = {"workload": f"synthetic VOI matrix {rows}x{cols} (PTV {n_ptv}), window {window}, density {density}, "
+                       f"D from {n_beams} 10x10 maps, gamma 1, eta 0.1, beam weight 0.1; BOO iterations"}
+    x0 = torch.full((cols,), 0.01, dtype=torch.float32, device="cuda")
+    for vt in ("f32", "f16", "bf16"):
+        A, AT = optimize.Matrix.synthetic(ctx, rows, cols, window, density, seed=seed, value_type=vt)
+        info = A.info()
+        P = optimize.Problem(ctx, A, AT, Dm, DTm, n_ptv, n_oar, w["max_dose"], w["max_weights"], w["min_dose"],
+                             w["min_weights"], w["oar_weights"], 1.0, 0.1)
+        bw = 0.1 * P.beam_weights_init(groups)
+        # SpMV alone: A x over the whole matrix
+        x = torch.rand(cols, device="cuda")
+        y = torch.empty(rows, device="cuda")
+        s = torch.cuda.current_stream()
+        for _ in range(3):
+            A.spmv(x, y, stream=s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 10
+        e0.record(s)
+        for _ in range(reps):
+            A.spmv(x, y, stream=s)
+        e1.record(s)
+        torch.cuda.synchronize()
+        spmv_ms = e0.elapsed_time(e1) / reps
+        vb = 4 if vt == "f32" else 2
+        spmv_bytes = info["nnz"] * (4 + vb) + (rows + 1) * 8 + cols * 4 + rows * 4
+        P.boo(groups, bw, x0, step_size=1e-3, iters=3, want=0, change_trigger=10 ** 9)  # warm-up
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = P.boo(groups, bw, x0, step_size=1e-3, iters=iters, want=0, change_trigger=10 ** 9)
+        dt = time.perf_counter() - t0
+        out[vt] = {"it_per_s": r["k"] / dt, "trials": r["trials"], "iters": r["k"], "loss": float(r["loss"][r["k"] - 1]),
+                   "nnz": info["nnz"], "matrix_bytes": info["device_bytes"],
+                   "spmv": {"ms": spmv_ms, "bytes": spmv_bytes, "gbs": spmv_bytes / spmv_ms * 1e-6,
+                            "frac": spmv_bytes / spmv_ms * 1e-6 / peak}}
+        del P, A, AT
+        torch.cuda.empty_cache()
+    for vt in ("f16", "bf16"):
+        out[vt]["speedup_vs_f32"] = out[vt]["it_per_s"] / out["f32"]["it_per_s"]
+        out[vt]["objective_rel_diff_vs_f32"] = abs(out[vt]["loss"] - out["f32"]["loss"]) / abs(out["f32"]["loss"])
+    return out
+
+
+def single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream, n_beams=20):
+    """The plain single-beam form: the same beams one DoseMatConstruction call
+    (one beam) at a time, as the reference's per-beam loop runs them."""
+    import torch
+
+    from fastdose_b200 import api
+
+    sel = beamlets[:n_beams]
+    for b in sel[:2]:
+        api.DoseMatConstruction(ctx, [b], fluence, dens, spec, kern, stream=stream).close()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for b in sel:
+        api.DoseMatConstruction(ctx, [b], fluence, dens, spec, kern, stream=stream).close()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    n = int(sum(len(b) for b in sel))
+    return {"beams": len(sel), "beamlets": n, "value": n / (e0.elapsed_time(e1) * 1e-3), "unit": UNIT}
+
+
 def run_fd2(args, rank, world):
     import torch
     import torch.distributed as dist
@@ -322,6 +411,11 @@ def run_fd2(args, rank, world):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
     }
+    if not args.no_extras:
+        sb = single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream)
+        sb["batched_speedup"] = value / world / sb["value"]
+        line["single_beam"] = sb
+        line["optimizer"] = optimizer_leg(ctx, args.opt_iters, args.opt_rows)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, os.cpu_count() or 1)
     if rank == 0:
@@ -337,7 +431,19 @@ def main():
     ap.add_argument("--beams", type=int, default=400)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the single-beam and optimizer legs")
+    ap.add_argument("--opt-iters", type=int, default=40)
+    ap.add_argument("--opt-rows", type=int, default=2_500_000)
+    ap.add_argument("--only-optimizer", action="store_true", help="run the optimizer leg alone (profiling)")
     args = ap.parse_args()
+    if args.only_optimizer:
+        import torch
+
+        from fastdose_b200 import api
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"optimizer": optimizer_leg(api.Context(0), args.opt_iters, args.opt_rows)}), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
