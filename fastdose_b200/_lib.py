@@ -55,14 +55,14 @@ _PROTOS = {
     "fd2_bev2pvcs_interp": (_i, [_vp, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "fd2_dose_compute_static": (_i, [_sz, _sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     # optimizer (fd2_opt.h)
-    "fd2_matrix_create": (_i, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _i, _vp]),
+    "fd2_matrix_create": (_i, [_vp, _i64, _i64, _i64, _vp, _vp, _vp, _i, _i, _vp]),
     "fd2_matrix_destroy": (_i, [_vp]),
     "fd2_matrix_info": (_i, [_vp, _vp]),
     "fd2_matrix_to_host": (_i, [_vp, _vp, _vp, _vp]),
     "fd2_matrix_transpose": (_i, [_vp, _vp]),
     "fd2_matrix_spmv": (_i, [_vp, _vp, _vp, _vp]),
-    "fd2_voi_matrices": (_i, [_vp, _vp, _i64, _i64, _i, _vp, _vp]),
-    "fd2_matrix_synthetic": (_i, [_vp, _i64, _i64, _i64, _f, _u64, _i, _vp, _vp]),
+    "fd2_voi_matrices": (_i, [_vp, _vp, _i64, _i64, _i, _i, _vp, _vp]),
+    "fd2_matrix_synthetic": (_i, [_vp, _i64, _i64, _i64, _f, _u64, _i, _i, _vp, _vp]),
     "fd2_fluence_grad": (_i, [_i, _vp, _vp, _vp, _vp, _vp, _vp]),
     "fd2_opt_problem_create": (_i, [_vp, _vp, _vp, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp]),
     "fd2_opt_problem_destroy": (_i, [_vp]),

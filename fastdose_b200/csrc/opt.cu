@@ -10,7 +10,7 @@
 // and the accelerated proximal-gradient loops BOO_IMRT_L2OneHalf_gpu_QL and
 // polish_BOO_IMRT_gpu (IMRTOpt/src/IMRTOptimize.cu:16-194, 391-476).
 //
-// Layout: the four matrices are merge-path CSR (spmv.cu); every vector is a
+// Layout: the four matrices are stream-SpMV CSR (spmv.cu); every vector is a
 // flat FP32 array.  The elementwise terms are one fused pass over the VOI and
 // D rows that also writes the gradient inputs; every sum (objective terms,
 // group norms, line-search terms) accumulates in FP64 through fixed-shape
@@ -218,7 +218,7 @@ __device__ __forceinline__ float as_float(T v) {
 // per beamlet: the sum of its PTV-row entries (AT rows list VOI columns
 // ascending, PTV first), scale applied
 template <typename T>
-__global__ void ptv_column_sums(const int64_t* __restrict__ off, const int32_t* __restrict__ col,
+__global__ void ptv_column_sums(const int64_t* __restrict__ off, ColView col,
                                 const T* __restrict__ val, const float* __restrict__ row_scale, int64_t rows,
                                 int64_t n_ptv, double* __restrict__ out) {
     const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
@@ -226,8 +226,8 @@ __global__ void ptv_column_sums(const int64_t* __restrict__ off, const int32_t* 
     if (r >= rows) return;
     double s = 0;
     for (int64_t k = off[r] + lane; k < off[r + 1]; k += 32) {
-        if (col[k] >= n_ptv) break;
-        s += (double)as_float(val[k]);
+        if (col.at(k) >= n_ptv) break;
+        s += (double)as_float(val[slot(k)]);
     }
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
     if (lane == 0) out[r] = s * (row_scale ? (double)row_scale[r] : 1.0);
@@ -529,15 +529,15 @@ int fd2_beam_weights_init(fd2_opt_problem* p, int64_t n_groups, const int64_t* h
     if (at->rows) {
         switch (at->value_type) {
             case FD2_VALUES_F16:
-                ptv_column_sums<__half><<<blocks, 256, 0, st>>>(at->d_off, at->d_col, (const __half*)at->d_val, rs,
+                ptv_column_sums<__half><<<blocks, 256, 0, st>>>(at->d_off, at->cols_view(), (const __half*)at->d_val, rs,
                                                                at->rows, p->n_ptv, d_s);
                 break;
             case FD2_VALUES_BF16:
                 ptv_column_sums<__nv_bfloat16><<<blocks, 256, 0, st>>>(
-                    at->d_off, at->d_col, (const __nv_bfloat16*)at->d_val, rs, at->rows, p->n_ptv, d_s);
+                    at->d_off, at->cols_view(), (const __nv_bfloat16*)at->d_val, rs, at->rows, p->n_ptv, d_s);
                 break;
             default:
-                ptv_column_sums<float><<<blocks, 256, 0, st>>>(at->d_off, at->d_col, (const float*)at->d_val, rs,
+                ptv_column_sums<float><<<blocks, 256, 0, st>>>(at->d_off, at->cols_view(), (const float*)at->d_val, rs,
                                                               at->rows, p->n_ptv, d_s);
         }
     }

@@ -2,25 +2,34 @@
 //
 // The reference multiplies with cusparseSpMV on 64-bit-index FP32 CSR
 // (IMRT::MatCSR64, IMRTOpt/include/IMRTDoseMat.cuh:29-69).  Here a matrix
-// holds int64 row offsets, int32 columns and FP32/FP16/BF16 values, and the
-// product is a merge-path SpMV: the sequence of row ends + nonzeros is cut
-// into equal tiles of kSpmvTile items, so every block streams the same number
-// of matrix bytes whatever the row lengths (VOI rows of a few hundred
-// nonzeros, beamlet rows of tens of thousands, empty rows).  A tile stages its
-// products val * x[col] in shared memory with independent, coalesced
-// streaming loads, each thread walks kSpmvItems items of the tile's merge
-// path, a block reduce-by-key scan joins the partial sums of rows that span
-// threads, and a second kernel adds the carries of rows that span tiles, in
-// tile order.  Summation order depends only on the matrix, so products are
-// reproducible run to run.  The product is HBM-bound: a pass reads
-// nnz * (value + 4-byte column) bytes plus the offsets, while x (a few hundred
-// KB to a few tens of MB) stays in L2.
+// holds int64 row offsets, int32 or packed 16-bit column indices and
+// FP32/FP16/BF16 values, and the product is a stream SpMV:
+//
+//  * the nonzeros are cut into chunks of 256 (32 lanes x 8); every warp owns
+//    a contiguous range of chunks, so every warp streams the same number of
+//    matrix bytes whatever the row lengths (VOI rows of a few hundred
+//    nonzeros, beamlet rows of tens of thousands, empty rows);
+//  * inside a chunk the nonzeros are stored lane-major (slot()), so a lane's
+//    two 16-byte streaming loads (`ld.global.cs`: the matrix is read once, x
+//    stays in the 126 MB L2) bring its 8 elements l, l+32, ..., l+224, and each
+//    x-gather of the warp covers 32 consecutive nonzeros;
+//  * rows are found from a row-start bitmap (1 bit per nonzero) and a per-chunk
+//    count of row starts: a 32-element slice without a row start is one FMA
+//    per lane into the open row; a slice with row starts closes the open row
+//    with a warp sum and sums the rows inside it with a segmented warp-shuffle
+//    scan -- no shared memory, no block barrier;
+//  * the row open at the end of a warp's range is carried; a second kernel
+//    adds carries in warp order.
+//
+// Summation order depends only on the matrix and the launch shape, so products
+// are reproducible run to run.  A pass is HBM-bound: it reads nnz x (value +
+// column) bytes, the bitmap (nnz/8 bytes) and x, and writes y.
 #include <algorithm>
 #include <cmath>
 #include <vector>
 
-#include <cub/block/block_scan.cuh>
 #include <cub/device/device_radix_sort.cuh>
+#include <cub/device/device_scan.cuh>
 
 #include "opt_internal.cuh"
 
@@ -28,141 +37,178 @@ namespace fd2 {
 
 namespace {
 
-__device__ __forceinline__ float load_value(const float* v, int64_t k) { return __ldcs(v + k); }
-__device__ __forceinline__ float load_value(const __half* v, int64_t k) {
-    return __half2float(__ushort_as_half(__ldcs(reinterpret_cast<const unsigned short*>(v) + k)));
-}
-__device__ __forceinline__ float load_value(const __nv_bfloat16* v, int64_t k) {
-    return __bfloat162float(__ushort_as_bfloat16(__ldcs(reinterpret_cast<const unsigned short*>(v) + k)));
-}
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kStreamThreads = 256;
+constexpr int kMaxStreamWarps = 148 * 64;  // one full wave of 64 warps per SM
 
-// Merge-path coordinate of a diagonal: rows consumed = the number of row ends
-// (offsets[1..rows]) that come before nonzero (diag - rows consumed).  A row
-// end is consumed before the nonzero with the same index.
-__global__ void spmv_plan_kernel(const int64_t* __restrict__ off, int64_t rows, int64_t nnz, int64_t n_tiles,
-                                 int64_t* __restrict__ tile_row, int64_t* __restrict__ tile_nz) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t > n_tiles) return;
-    const int64_t diag = min(t * (int64_t)kSpmvTile, rows + nnz);
-    int64_t lo = max(diag - nnz, (int64_t)0), hi = min(diag, rows);
-    while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (off[mid + 1] <= diag - 1 - mid)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    tile_row[t] = lo;
-    tile_nz[t] = diag - lo;
-}
-
-struct RowCarry {
-    int key;  // tile-relative row
-    float value;
+struct StreamArgs {
+    const void* val;
+    ColView cols;
+    const uint32_t* head;
+    const int32_t* chunk_h;
+    const int32_t* nzrow;
+    const float* row_scale;
+    int64_t n_chunks;
+    int n_warps;
+    int64_t rows;
+    int64_t* carry_row;
+    float* carry_val;
 };
 
-struct CarryJoin {  // reduce-by-key: sums runs of equal keys
-    __device__ __forceinline__ RowCarry operator()(const RowCarry& a, const RowCarry& b) const {
-        return b.key == a.key ? RowCarry{b.key, a.value + b.value} : b;
-    }
-};
-
-template <typename T>
-__global__ void __launch_bounds__(kSpmvThreads) spmv_tile_kernel(
-    const int64_t* __restrict__ off, const int32_t* __restrict__ col, const T* __restrict__ val,
-    const float* __restrict__ x, const float* __restrict__ row_scale, const int64_t* __restrict__ tile_row,
-    const int64_t* __restrict__ tile_nz, float* __restrict__ y, int64_t* __restrict__ carry_row,
-    float* __restrict__ carry_val) {
-    __shared__ float s_prod[kSpmvTile];
-    __shared__ int s_rowend[kSpmvTile + 1];
-    typedef cub::BlockScan<RowCarry, kSpmvThreads> Scan;
-    __shared__ typename Scan::TempStorage scan_tmp;
-
-    const int64_t t = blockIdx.x;
-    const int64_t r0 = tile_row[t], z0 = tile_nz[t];
-    const int nr = (int)(tile_row[t + 1] - r0), nz = (int)(tile_nz[t + 1] - z0);
-
-    // stage the tile's row ends (relative to z0) and products
-    for (int i = threadIdx.x; i < nr; i += kSpmvThreads) s_rowend[i] = (int)(off[r0 + i + 1] - z0);
-    if (threadIdx.x == 0) s_rowend[nr] = nz + 1;  // the row in progress at the tile end does not end here
-    {
-        int c[kSpmvItems];
-        float v[kSpmvItems];
+// 8 consecutive values of a lane (16-byte aligned: k is a multiple of 8)
+__device__ __forceinline__ void load8(const float* v, int64_t k, float (&o)[8]) {
+    const float4* p = reinterpret_cast<const float4*>(v + k);
+    const float4 a = __ldcs(p), b = __ldcs(p + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+    o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+__device__ __forceinline__ void load8(const __half* v, int64_t k, float (&o)[8]) {
+    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(v + k));
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
 #pragma unroll
-        for (int u = 0; u < kSpmvItems; u++) {
-            const int j = u * kSpmvThreads + threadIdx.x;
-            c[u] = 0;
-            v[u] = 0.0f;
-            if (j < nz) {
-                c[u] = __ldcs(col + z0 + j);
-                v[u] = load_value(val, z0 + j);
+    for (int i = 0; i < 4; i++) {
+        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
+        o[2 * i] = f.x;
+        o[2 * i + 1] = f.y;
+    }
+}
+__device__ __forceinline__ void load8(const __nv_bfloat16* v, int64_t k, float (&o)[8]) {
+    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(v + k));
+    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[i]));
+        o[2 * i] = f.x;
+        o[2 * i + 1] = f.y;
+    }
+}
+
+__device__ __forceinline__ void load_i32x8(const int32_t* c, int64_t k, int (&o)[8]) {
+    const int4* p = reinterpret_cast<const int4*>(c + k);
+    const int4 a = __ldcs(p), b = __ldcs(p + 1);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+    o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
+}
+
+template <bool kPacked>
+__device__ __forceinline__ void load_cols8(const ColView& cv, int64_t chunk, int lane, int (&o)[8]) {
+    const int64_t k = chunk * kChunk + 8 * lane;
+    if constexpr (!kPacked) {
+        load_i32x8(cv.col, k, o);
+    } else {
+        const int32_t base = __ldg(cv.cbase + chunk);  // one address for the warp
+        if (base >= 0) {
+            const uint4 u = __ldcs(reinterpret_cast<const uint4*>(cv.col16 + k));
+            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                o[2 * i] = base + (int)(w[i] & 0xffffu);
+                o[2 * i + 1] = base + (int)(w[i] >> 16);
             }
-        }
-#pragma unroll
-        for (int u = 0; u < kSpmvItems; u++) {
-            const int j = u * kSpmvThreads + threadIdx.x;
-            if (j < nz) s_prod[j] = v[u] * __ldg(x + c[u]);
-        }
-    }
-    __syncthreads();
-
-    // this thread's stretch of the tile's merge path
-    const int total = nr + nz;
-    const int diag = min((int)threadIdx.x * kSpmvItems, total);
-    const int dend = min(diag + kSpmvItems, total);
-    int lo = max(diag - nz, 0), hi = min(diag, nr);
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (s_rowend[mid] <= diag - 1 - mid)
-            lo = mid + 1;
-        else
-            hi = mid;
-    }
-    int i = lo, j = diag - lo;
-    float run = 0.0f, first_val = 0.0f;
-    int first_row = -1;
-    for (int it = diag; it < dend; it++) {
-        if (j < s_rowend[i]) {
-            run += s_prod[j];
-            j++;
         } else {
-            if (first_row < 0) {
-                first_row = i;
-                first_val = run;
-            } else {
-                const int64_t r = r0 + i;
-                y[r] = row_scale ? row_scale[r] * run : run;
-            }
-            run = 0.0f;
-            i++;
+            load_i32x8(cv.exc, (int64_t)(-1 - base) * kChunk + 8 * lane, o);
         }
-    }
-    // the first row this thread ends also holds the trailing partial sums of
-    // the threads before it that carried the same row
-    RowCarry mine{i, run}, prefix, total_carry;
-    Scan(scan_tmp).ExclusiveScan(mine, prefix, RowCarry{-1, 0.0f}, CarryJoin(), total_carry);
-    if (first_row >= 0) {
-        const float v = first_val + (prefix.key == first_row ? prefix.value : 0.0f);
-        const int64_t r = r0 + first_row;
-        y[r] = row_scale ? row_scale[r] * v : v;
-    }
-    if (threadIdx.x == 0) {
-        carry_row[t] = r0 + total_carry.key;
-        carry_val[t] = total_carry.value;
     }
 }
 
-// Adds the carries of rows that span tiles: the first tile of each run of
-// equal carry rows sums the run in tile order.
-__global__ void spmv_fixup_kernel(int64_t n_tiles, const int64_t* __restrict__ carry_row,
+__device__ __forceinline__ void put(float* y, const float* rs, int r, float v) { y[r] = rs ? rs[r] * v : v; }
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// One warp per contiguous range of chunks.  In a chunk, slice i holds logical
+// elements 32 i .. 32 i + 31 (one per lane); word i of the row-start bitmap
+// flags the lanes that start a row.  A slice without row starts only adds to
+// the open row (one FMA per lane); a slice with row starts closes the open row
+// (warp sum), sums the rows that start and end inside it with a segmented
+// warp scan, and leaves its last row open.
+template <typename T, bool kPacked>
+__global__ void __launch_bounds__(kStreamThreads) spmv_stream_kernel(StreamArgs a, const float* __restrict__ x,
+                                                                     float* __restrict__ y) {
+    const int lane = threadIdx.x & 31;
+    const int w = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
+    if (w >= a.n_warps) return;  // uniform per warp
+    const int64_t c0 = (int64_t)w * a.n_chunks / a.n_warps, c1 = (int64_t)(w + 1) * a.n_chunks / a.n_warps;
+    const T* __restrict__ val = static_cast<const T*>(a.val);
+    float oacc = 0.0f;        // this lane's share of the open row (the row in progress), this warp's part
+    bool open_valid = false;  // the warp has met an element of the open row
+    int open_row = 0;
+    if (c0 < c1) {
+        const int hb0 = __ldg(a.chunk_h + c0);
+        if (hb0 > 0 && !(__ldg(a.head + c0 * kChunkWords) & 1u)) open_row = __ldg(a.nzrow + hb0 - 1);
+    }
+    for (int64_t c = c0; c < c1; c++) {
+        float v[8];
+        int col[8];
+        load8(val, c * kChunk + 8 * lane, v);
+        load_cols8<kPacked>(a.cols, c, lane, col);
+        const uint4 h0 = __ldg(reinterpret_cast<const uint4*>(a.head + c * kChunkWords));
+        const uint4 h1 = __ldg(reinterpret_cast<const uint4*>(a.head + c * kChunkWords) + 1);
+        const uint32_t hw[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+        if (!(h0.x | h0.y | h0.z | h0.w | h1.x | h1.y | h1.z | h1.w)) {  // no row starts: all of it is the open row
+#pragma unroll
+            for (int i = 0; i < 8; i++) oacc = fmaf(v[i], __ldg(x + col[i]), oacc);
+            open_valid = true;
+            continue;
+        }
+        const int hbase = __ldg(a.chunk_h + c);
+        int hcnt = 0;
+#pragma unroll
+        for (int i = 0; i < 8; i++) {
+            const float p = v[i] * __ldg(x + col[i]);
+            const uint32_t m = hw[i];
+            if (m == 0) {
+                oacc += p;
+                open_valid = true;
+                continue;
+            }
+            // close the open row: its lanes' shares plus the lanes before the first start
+            const int fh = __ffs(m) - 1;
+            const float closing = warp_sum(oacc + (lane < fh ? p : 0.0f));
+            if ((open_valid || fh > 0) && lane == 0) put(y, a.row_scale, open_row, closing);
+            // rows inside the slice: segmented inclusive scan from the first start
+            float s = lane >= fh ? p : 0.0f;
+            int f = (m >> lane) & 1u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const float ts = __shfl_up_sync(kFull, s, o);
+                const int tf = __shfl_up_sync(kFull, f, o);
+                if (lane >= o) {
+                    if (!f) s += ts;
+                    f |= tf;
+                }
+            }
+            if (lane < 31 && lane >= fh && ((m >> (lane + 1)) & 1u))
+                put(y, a.row_scale, __ldg(a.nzrow + hbase + hcnt + __popc(m & ((2u << lane) - 1u)) - 1), s);
+            // the slice's last row stays open
+            const int lh = 31 - __clz(m);
+            oacc = lane >= lh ? p : 0.0f;
+            hcnt += __popc(m);
+            open_row = __ldg(a.nzrow + hbase + hcnt - 1);
+            open_valid = true;
+        }
+    }
+    const float part = warp_sum(oacc);
+    if (lane == 0) {
+        a.carry_row[w] = open_valid ? (int64_t)open_row : a.rows;
+        a.carry_val[w] = part;
+    }
+}
+
+// Adds the carries of rows that cross warp ranges: the first warp of each run
+// of equal carry rows sums the run in warp order.
+__global__ void spmv_fixup_kernel(int n_warps, const int64_t* __restrict__ carry_row,
                                   const float* __restrict__ carry_val, const float* __restrict__ row_scale,
                                   int64_t rows, float* __restrict__ y) {
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (t >= n_tiles) return;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_warps) return;
     const int64_t r = carry_row[t];
     if (r >= rows || (t > 0 && carry_row[t - 1] == r)) return;
     float s = 0.0f;
-    for (int64_t u = t; u < n_tiles && carry_row[u] == r; u++) s += carry_val[u];
+    for (int u = t; u < n_warps && carry_row[u] == r; u++) s += carry_val[u];
     y[r] += row_scale ? row_scale[r] * s : s;
 }
 
@@ -172,7 +218,110 @@ __global__ void scale_vector_kernel(const float* __restrict__ s, const float* __
         out[i] = s[i] * x[i];
 }
 
-// ---------------------------------------------------------------- creation
+// ---------------------------------------------------------------- plan
+unsigned grid_for(int64_t n, int threads = 256) {
+    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 16));
+}
+
+// bit off[r] of the row-start bitmap for every row with nonzeros (rows own
+// distinct bits; atomicOr makes the word updates safe)
+__global__ void mark_row_starts(const int64_t* __restrict__ off, int64_t rows, uint32_t* __restrict__ head,
+                                int32_t* __restrict__ nonempty) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
+        const bool ne = off[r + 1] > off[r];
+        nonempty[r] = ne;
+        if (ne) atomicOr(head + off[r] / 32, 1u << (off[r] % 32));
+    }
+}
+
+__global__ void scatter_rows(const int32_t* __restrict__ nonempty, const int32_t* __restrict__ pos, int64_t rows,
+                             int32_t* __restrict__ nzrow) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x)
+        if (nonempty[r]) nzrow[pos[r]] = (int32_t)r;
+}
+
+__global__ void chunk_head_counts(const uint32_t* __restrict__ head, int64_t n_chunks, int32_t* __restrict__ cnt) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n_chunks;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        int s = 0;
+#pragma unroll
+        for (int i = 0; i < kChunkWords; i++) s += __popc(head[c * kChunkWords + i]);
+        cnt[c] = s;
+    }
+}
+
+// PACKED16, pass 1: one warp per chunk; is the chunk's column span < 65536?
+__global__ void chunk_span(const int32_t* __restrict__ col, int64_t nnz, int64_t n_chunks, int32_t* __restrict__ base,
+                           int32_t* __restrict__ wide) {
+    const int64_t c = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (c >= n_chunks) return;
+    int lo = 0x7fffffff, hi = -1;
+    for (int i = lane; i < kChunk; i += 32) {
+        const int64_t k = c * kChunk + i;
+        if (k < nnz) {
+            lo = min(lo, col[k]);
+            hi = max(hi, col[k]);
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(kFull, lo, o));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, o));
+    }
+    if (lane == 0) {
+        if (hi < 0) lo = hi = 0;  // chunk of padding only
+        base[c] = lo;
+        wide[c] = hi - lo > 0xffff;
+    }
+}
+
+// PACKED16, pass 2: offsets for narrow chunks, int32 copies for wide ones,
+// from logical-order columns into storage order
+__global__ void pack_columns(const int32_t* __restrict__ col, int64_t nnz, int64_t n_chunks,
+                             const int32_t* __restrict__ wide, const int32_t* __restrict__ exc_slot,
+                             int32_t* __restrict__ base, uint16_t* __restrict__ col16, int32_t* __restrict__ exc) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n_chunks * kChunk;
+         k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t c = k / kChunk, q = slot(k);
+        const int cv = k < nnz ? col[k] : 0;
+        if (wide[c]) {
+            exc[(int64_t)exc_slot[c] * kChunk + q % kChunk] = cv;
+            col16[q] = 0;
+        } else {
+            col16[q] = (uint16_t)(k < nnz ? cv - base[c] : 0);
+        }
+    }
+}
+
+// logical order -> storage order
+template <typename E>
+__global__ void to_storage_order(const E* __restrict__ src, E* __restrict__ dst, int64_t n) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+        dst[slot(k)] = src[k];
+}
+
+__global__ void mark_wide_bases(const int32_t* __restrict__ wide, const int32_t* __restrict__ slot, int64_t n_chunks,
+                                int32_t* __restrict__ base) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n_chunks;
+         c += (int64_t)gridDim.x * blockDim.x)
+        if (wide[c]) base[c] = -1 - slot[c];
+}
+
+template <typename T>
+int exclusive_scan(const T* in, T* out, int64_t n, cudaStream_t st) {
+    if (n <= 0) return FD2_OK;
+    size_t tb = 0;
+    FD2_CHECK_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, in, out, n, st));
+    void* tmp = nullptr;
+    FD2_CHECK_CUDA(cudaMalloc(&tmp, std::max<size_t>(tb, 16)));
+    cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tb, in, out, n, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(tmp);
+    FD2_CHECK_CUDA(e);
+    return FD2_OK;
+}
+
+// ---------------------------------------------------------------- set-up kernels
 __global__ void abs_max_by_column(const int32_t* __restrict__ col, const float* __restrict__ v, int64_t nnz,
                                   unsigned* __restrict__ mx) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x)
@@ -196,6 +345,9 @@ template <>
 __device__ __forceinline__ __nv_bfloat16 from_float<__nv_bfloat16>(float v) {
     return __float2bfloat16_rn(v);
 }
+__device__ __forceinline__ float to_float(float v) { return v; }
+__device__ __forceinline__ float to_float(__half v) { return __half2float(v); }
+__device__ __forceinline__ float to_float(__nv_bfloat16 v) { return __bfloat162float(v); }
 
 template <typename T>
 __global__ void quantize_by_column(const int32_t* __restrict__ col, const float* __restrict__ v,
@@ -214,22 +366,23 @@ __device__ __forceinline__ int64_t row_of(const int64_t* __restrict__ off, int64
     return lo;
 }
 
-// to FP32 with the scale applied
+// columns (decoded) and values as FP32 with the scale applied
 template <typename T>
-__global__ void dequantize(const int64_t* __restrict__ off, int64_t rows, const int32_t* __restrict__ col,
-                           const T* __restrict__ val, const float* __restrict__ s, int axis, int64_t nnz,
-                           float* __restrict__ out) {
+__global__ void unpack_entries(const int64_t* __restrict__ off, int64_t rows, ColView cv, const T* __restrict__ val,
+                               const float* __restrict__ s, int axis, int64_t nnz, int32_t* __restrict__ col_out,
+                               float* __restrict__ val_out) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
-        float v = load_value(val, k);
+        const int c = cv.at(k);
+        float v = to_float(val[slot(k)]);
         if (axis == FD2_SCALE_COLS)
-            v *= s[col[k]];
+            v *= s[c];
         else if (axis == FD2_SCALE_ROWS)
             v *= s[row_of(off, rows, k)];
-        out[k] = v;
+        if (col_out) col_out[k] = c;
+        if (val_out) val_out[k] = v;
     }
 }
 
-// ---------------------------------------------------------------- transpose
 __global__ void iota64(int64_t* __restrict__ p, int64_t n) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
         p[k] = k;
@@ -256,23 +409,23 @@ __global__ void gather_transposed(const int64_t* __restrict__ off, int64_t rows,
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
         const int64_t src = perm[k];
         col_out[k] = (int32_t)row_of(off, rows, src);
-        val_out[k] = val[src];
+        val_out[k] = val[slot(src)];
     }
 }
 
-unsigned grid_for(int64_t n, int threads = 256) {
-    return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 16));
-}
-
 template <typename T>
-int launch_spmv(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) {
-    const float* rs = m->scale_axis == FD2_SCALE_ROWS ? m->d_scale : nullptr;
-    spmv_tile_kernel<T><<<(unsigned)m->n_tiles, kSpmvThreads, 0, st>>>(
-        m->d_off, m->d_col, (const T*)m->d_val, x, rs, m->d_tile_row, m->d_tile_nz, y, m->d_carry_row,
-        m->d_carry_val);
+int launch_stream(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) {
+    StreamArgs a{m->d_val, m->cols_view(), m->d_head, m->d_chunk_h, m->d_nzrow,
+                 m->scale_axis == FD2_SCALE_ROWS ? m->d_scale : nullptr, m->n_chunks, m->n_warps, m->rows,
+                 m->d_carry_row, m->d_carry_val};
+    const unsigned blocks = (unsigned)(((int64_t)m->n_warps * 32 + kStreamThreads - 1) / kStreamThreads);
+    if (m->index_format == FD2_INDEX_PACKED16)
+        spmv_stream_kernel<T, true><<<blocks, kStreamThreads, 0, st>>>(a, x, y);
+    else
+        spmv_stream_kernel<T, false><<<blocks, kStreamThreads, 0, st>>>(a, x, y);
     FD2_CHECK_CUDA(cudaGetLastError());
-    spmv_fixup_kernel<<<grid_for(m->n_tiles), 256, 0, st>>>(m->n_tiles, m->d_carry_row, m->d_carry_val, rs, m->rows,
-                                                             y);
+    spmv_fixup_kernel<<<(m->n_warps + 255) / 256, 256, 0, st>>>(m->n_warps, m->d_carry_row, m->d_carry_val,
+                                                               a.row_scale, m->rows, y);
     FD2_CHECK_CUDA(cudaGetLastError());
     return FD2_OK;
 }
@@ -280,24 +433,28 @@ int launch_spmv(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) 
 template <typename T>
 int transpose_typed(const fd2_matrix* m, fd2_matrix* t, cudaStream_t st) {
     const int64_t nnz = m->nnz;
-    int32_t* keys_out = nullptr;
+    int32_t *keys_in = nullptr, *keys_out = nullptr;
     int64_t *perm_in = nullptr, *perm_out = nullptr;
     void* tmp = nullptr;
     size_t tmp_bytes = 0;
     int end_bit = 1;
     while (end_bit < 31 && ((int64_t)1 << end_bit) < m->cols) end_bit++;
     int rc = FD2_OK;
-    cudaError_t e = cudaMalloc(&keys_out, nnz * sizeof(int32_t));
+    cudaError_t e = cudaMalloc(&keys_in, nnz * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&keys_out, nnz * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&perm_in, nnz * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMalloc(&perm_out, nnz * sizeof(int64_t));
-    if (e == cudaSuccess)
-        e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, m->d_col, keys_out, perm_in, perm_out, nnz, 0, end_bit,
+    if (e == cudaSuccess) {
+        unpack_entries<T><<<grid_for(nnz), 256, 0, st>>>(m->d_off, m->rows, m->cols_view(), (const T*)m->d_val,
+                                                         nullptr, FD2_SCALE_NONE, nnz, keys_in, nullptr);
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, keys_in, keys_out, perm_in, perm_out, nnz, 0, end_bit,
                                             st);
-    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 16));
     if (e == cudaSuccess) {
         // stable sort by column: within a new row, entries keep ascending old-row order
         iota64<<<grid_for(nnz), 256, 0, st>>>(perm_in, nnz);
-        e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, m->d_col, keys_out, perm_in, perm_out, nnz, 0, end_bit,
+        e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, keys_in, keys_out, perm_in, perm_out, nnz, 0, end_bit,
                                             st);
     }
     if (e == cudaSuccess) {
@@ -311,17 +468,27 @@ int transpose_typed(const fd2_matrix* m, fd2_matrix* t, cudaStream_t st) {
         set_error("matrix_transpose: %s", cudaGetErrorString(e));
         rc = e == cudaErrorMemoryAllocation ? FD2_ERR_OUT_OF_MEMORY : FD2_ERR_CUDA;
     }
-    for (void* p : {(void*)keys_out, (void*)perm_in, (void*)perm_out, tmp})
+    for (void* p : {(void*)keys_in, (void*)keys_out, (void*)perm_in, (void*)perm_out, tmp})
         if (p) cudaFree(p);
     return rc;
 }
 
 }  // namespace
 
-int matrix_alloc(fd2_matrix* m) {
+int matrix_alloc(fd2_matrix* m, cudaStream_t st) {
     FD2_CHECK_CUDA(cudaMalloc(&m->d_off, (m->rows + 1) * sizeof(int64_t)));
-    FD2_CHECK_CUDA(cudaMalloc(&m->d_col, std::max<int64_t>(m->nnz, 1) * sizeof(int32_t)));
-    FD2_CHECK_CUDA(cudaMalloc(&m->d_val, std::max<int64_t>(m->nnz, 1) * value_size(m->value_type)));
+    return matrix_alloc_entries(m, st);
+}
+
+int matrix_alloc_entries(fd2_matrix* m, cudaStream_t st) {
+    const int64_t pad = round_chunk(m->nnz);
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_col, std::max<int64_t>(pad, 1) * sizeof(int32_t)));
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_val, std::max<int64_t>(pad, 1) * value_size(m->value_type)));
+    if (pad > m->nnz) {  // the last chunk's padding: column 0, value 0
+        FD2_CHECK_CUDA(cudaMemsetAsync(m->d_col + m->nnz, 0, (pad - m->nnz) * sizeof(int32_t), st));
+        FD2_CHECK_CUDA(cudaMemsetAsync((char*)m->d_val + m->nnz * value_size(m->value_type), 0,
+                                       (pad - m->nnz) * value_size(m->value_type), st));
+    }
     if (m->scale_axis != FD2_SCALE_NONE) {
         const int64_t n = m->scale_axis == FD2_SCALE_ROWS ? m->rows : m->cols;
         FD2_CHECK_CUDA(cudaMalloc(&m->d_scale, std::max<int64_t>(n, 1) * sizeof(float)));
@@ -330,34 +497,171 @@ int matrix_alloc(fd2_matrix* m) {
 }
 
 void matrix_free(fd2_matrix* m) {
-    for (void* p : {(void*)m->d_off, (void*)m->d_col, m->d_val, (void*)m->d_scale, (void*)m->d_tile_row,
-                    (void*)m->d_tile_nz, (void*)m->d_carry_row, (void*)m->d_carry_val, (void*)m->d_xs})
+    for (void* p : {(void*)m->d_off, (void*)m->d_col, (void*)m->d_col16, (void*)m->d_cbase, (void*)m->d_exc, m->d_val,
+                    (void*)m->d_scale, (void*)m->d_head, (void*)m->d_chunk_h, (void*)m->d_nzrow,
+                    (void*)m->d_carry_row, (void*)m->d_carry_val, (void*)m->d_xs})
         if (p) cudaFree(p);
     m->d_off = nullptr;
     m->d_col = nullptr;
+    m->d_col16 = nullptr;
+    m->d_cbase = m->d_exc = nullptr;
     m->d_val = nullptr;
     m->d_scale = nullptr;
-    m->d_tile_row = m->d_tile_nz = m->d_carry_row = nullptr;
+    m->d_head = nullptr;
+    m->d_chunk_h = m->d_nzrow = nullptr;
+    m->d_carry_row = nullptr;
     m->d_carry_val = m->d_xs = nullptr;
 }
 
-int matrix_plan(fd2_matrix* m, cudaStream_t st) {
-    const int64_t items = m->rows + m->nnz;
-    m->n_tiles = (items + kSpmvTile - 1) / kSpmvTile;
-    FD2_CHECK_CUDA(cudaMalloc(&m->d_tile_row, (m->n_tiles + 1) * sizeof(int64_t)));
-    FD2_CHECK_CUDA(cudaMalloc(&m->d_tile_nz, (m->n_tiles + 1) * sizeof(int64_t)));
-    FD2_CHECK_CUDA(cudaMalloc(&m->d_carry_row, std::max<int64_t>(m->n_tiles, 1) * sizeof(int64_t)));
-    FD2_CHECK_CUDA(cudaMalloc(&m->d_carry_val, std::max<int64_t>(m->n_tiles, 1) * sizeof(float)));
+// Warps of one full wave of the stream kernel for this matrix's instance: every
+// warp owns one contiguous range, so there is no second, partial wave.
+template <typename T, bool kPacked>
+int resident_warps(int sm_count) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_stream_kernel<T, kPacked>, kStreamThreads, 0) !=
+            cudaSuccess ||
+        per_sm < 1)
+        per_sm = 1;
+    return per_sm * sm_count * (kStreamThreads / 32);
+}
+
+int stream_warps(const fd2_matrix* m) {
+    const int sms = m->ctx->sm_count > 0 ? m->ctx->sm_count : 148;
+    const bool pk = m->index_format == FD2_INDEX_PACKED16;
+    int w;
+    switch (m->value_type) {
+        case FD2_VALUES_F16: w = pk ? resident_warps<__half, true>(sms) : resident_warps<__half, false>(sms); break;
+        case FD2_VALUES_BF16:
+            w = pk ? resident_warps<__nv_bfloat16, true>(sms) : resident_warps<__nv_bfloat16, false>(sms);
+            break;
+        default: w = pk ? resident_warps<float, true>(sms) : resident_warps<float, false>(sms);
+    }
+    return std::min(w, kMaxStreamWarps);
+}
+
+int matrix_finalize(fd2_matrix* m, cudaStream_t st) {
+    m->n_chunks = round_chunk(m->nnz) / kChunk;
+    m->n_warps = (int)std::max<int64_t>(1, std::min<int64_t>(m->n_chunks, stream_warps(m)));
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_head, std::max<int64_t>(m->n_chunks * kChunkWords, 1) * sizeof(uint32_t)));
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_chunk_h, std::max<int64_t>(m->n_chunks, 1) * sizeof(int32_t)));
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_carry_row, m->n_warps * sizeof(int64_t)));
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_carry_val, m->n_warps * sizeof(float)));
     if (m->scale_axis == FD2_SCALE_COLS)
         FD2_CHECK_CUDA(cudaMalloc(&m->d_xs, std::max<int64_t>(m->cols, 1) * sizeof(float)));
-    spmv_plan_kernel<<<(unsigned)((m->n_tiles + 1 + 255) / 256), 256, 0, st>>>(m->d_off, m->rows, m->nnz, m->n_tiles,
-                                                                              m->d_tile_row, m->d_tile_nz);
-    FD2_CHECK_CUDA(cudaGetLastError());
-    return FD2_OK;
+    FD2_CHECK_CUDA(cudaMemsetAsync(m->d_head, 0, std::max<int64_t>(m->n_chunks * kChunkWords, 1) * sizeof(uint32_t),
+                                   st));
+    // row starts, non-empty rows, row starts before each chunk
+    int32_t *ne = nullptr, *pos = nullptr, *cnt = nullptr;
+    auto cleanup = [&]() {
+        for (void* p : {(void*)ne, (void*)pos, (void*)cnt})
+            if (p) cudaFree(p);
+    };
+    const int64_t rows1 = std::max<int64_t>(m->rows, 1);
+    if (cudaMalloc(&ne, rows1 * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&pos, rows1 * sizeof(int32_t)) != cudaSuccess ||
+        cudaMalloc(&cnt, std::max<int64_t>(m->n_chunks, 1) * sizeof(int32_t)) != cudaSuccess) {
+        cleanup();
+        set_error("matrix_finalize: out of device memory");
+        return FD2_ERR_OUT_OF_MEMORY;
+    }
+    int rc = FD2_OK;
+    if (m->rows) mark_row_starts<<<grid_for(m->rows), 256, 0, st>>>(m->d_off, m->rows, m->d_head, ne);
+    if (m->rows) rc = exclusive_scan(ne, pos, m->rows, st);
+    int32_t last_ne = 0, last_pos = 0;
+    if (!rc && m->rows) {
+        if (cudaMemcpy(&last_ne, ne + m->rows - 1, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+            cudaMemcpy(&last_pos, pos + m->rows - 1, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = FD2_ERR_CUDA;
+    }
+    m->n_nzrows = (int64_t)last_pos + last_ne;
+    if (!rc && cudaMalloc(&m->d_nzrow, std::max<int64_t>(m->n_nzrows, 1) * sizeof(int32_t)) != cudaSuccess)
+        rc = FD2_ERR_OUT_OF_MEMORY;
+    if (!rc && m->rows) scatter_rows<<<grid_for(m->rows), 256, 0, st>>>(ne, pos, m->rows, m->d_nzrow);
+    if (!rc && m->n_chunks) {
+        chunk_head_counts<<<grid_for(m->n_chunks), 256, 0, st>>>(m->d_head, m->n_chunks, cnt);
+        rc = exclusive_scan(cnt, m->d_chunk_h, m->n_chunks, st);
+    }
+    // 16-bit column packing
+    if (!rc && m->index_format == FD2_INDEX_PACKED16 && m->n_chunks) {
+        int32_t *wide = ne, *eslot = pos;  // reuse when large enough
+        bool own = m->n_chunks > rows1;
+        if (own && (cudaMalloc(&wide, m->n_chunks * sizeof(int32_t)) != cudaSuccess ||
+                    cudaMalloc(&eslot, m->n_chunks * sizeof(int32_t)) != cudaSuccess))
+            rc = FD2_ERR_OUT_OF_MEMORY;
+        if (!rc && cudaMalloc(&m->d_cbase, m->n_chunks * sizeof(int32_t)) != cudaSuccess) rc = FD2_ERR_OUT_OF_MEMORY;
+        if (!rc) {
+            chunk_span<<<(unsigned)((m->n_chunks * 32 + 255) / 256), 256, 0, st>>>(m->d_col, m->nnz, m->n_chunks,
+                                                                                 m->d_cbase, wide);
+            rc = exclusive_scan(wide, eslot, m->n_chunks, st);
+        }
+        int32_t lw = 0, ls = 0;
+        if (!rc && (cudaMemcpy(&lw, wide + m->n_chunks - 1, 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
+                    cudaMemcpy(&ls, eslot + m->n_chunks - 1, 4, cudaMemcpyDeviceToHost) != cudaSuccess))
+            rc = FD2_ERR_CUDA;
+        m->n_exc = (int64_t)lw + ls;
+        if (!rc && (cudaMalloc(&m->d_col16, m->n_chunks * kChunk * sizeof(uint16_t)) != cudaSuccess ||
+                    cudaMalloc(&m->d_exc, std::max<int64_t>(m->n_exc, 1) * kChunk * sizeof(int32_t)) != cudaSuccess))
+            rc = FD2_ERR_OUT_OF_MEMORY;
+        if (!rc) {
+            pack_columns<<<grid_for(m->n_chunks * kChunk), 256, 0, st>>>(m->d_col, m->nnz, m->n_chunks, wide, eslot,
+                                                                        m->d_cbase, m->d_col16, m->d_exc);
+            mark_wide_bases<<<grid_for(m->n_chunks), 256, 0, st>>>(wide, eslot, m->n_chunks, m->d_cbase);
+            if (cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
+        }
+        if (own) {
+            if (wide) cudaFree(wide);
+            if (eslot) cudaFree(eslot);
+        }
+        if (!rc) {  // the int32 columns are no longer needed
+            cudaFree(m->d_col);
+            m->d_col = nullptr;
+        }
+    } else if (!rc && m->index_format == FD2_INDEX_PACKED16) {
+        cudaFree(m->d_col);  // empty matrix: nothing to pack
+        m->d_col = nullptr;
+        if (cudaMalloc(&m->d_cbase, sizeof(int32_t)) != cudaSuccess ||
+            cudaMalloc(&m->d_col16, kChunk * sizeof(uint16_t)) != cudaSuccess ||
+            cudaMalloc(&m->d_exc, kChunk * sizeof(int32_t)) != cudaSuccess)
+            rc = FD2_ERR_OUT_OF_MEMORY;
+    }
+    // values (and int32 columns) to storage order
+    if (!rc && m->n_chunks) {
+        const int64_t pad = m->n_chunks * kChunk;
+        const size_t vs = value_size(m->value_type);
+        void* tmp = nullptr;
+        if (cudaMalloc(&tmp, pad * vs) != cudaSuccess) {
+            rc = FD2_ERR_OUT_OF_MEMORY;
+        } else {
+            if (vs == 4)
+                to_storage_order<uint32_t><<<grid_for(pad), 256, 0, st>>>((const uint32_t*)m->d_val, (uint32_t*)tmp, pad);
+            else
+                to_storage_order<uint16_t><<<grid_for(pad), 256, 0, st>>>((const uint16_t*)m->d_val, (uint16_t*)tmp, pad);
+            if (cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
+            cudaFree(m->d_val);
+            m->d_val = tmp;
+        }
+        if (!rc && m->d_col) {
+            int32_t* tc = nullptr;
+            if (cudaMalloc(&tc, pad * sizeof(int32_t)) != cudaSuccess) {
+                rc = FD2_ERR_OUT_OF_MEMORY;
+            } else {
+                to_storage_order<int32_t><<<grid_for(pad), 256, 0, st>>>(m->d_col, tc, pad);
+                if (cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
+                cudaFree(m->d_col);
+                m->d_col = tc;
+            }
+        }
+    }
+    if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    cleanup();
+    if (rc && rc != FD2_ERR_OUT_OF_MEMORY) set_error("matrix_finalize: %s", cudaGetErrorString(cudaGetLastError()));
+    return rc;
 }
 
 int matrix_spmv(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) {
     if (m->rows == 0) return FD2_OK;
+    FD2_CHECK_CUDA(cudaMemsetAsync(y, 0, m->rows * sizeof(float), st));  // empty rows, and rows only carries reach
+    if (m->n_chunks == 0) return FD2_OK;
     if (m->scale_axis == FD2_SCALE_COLS) {
         scale_vector_kernel<<<grid_for(m->cols), 256, 0, st>>>(m->d_scale, x, m->d_xs, m->cols);
         FD2_CHECK_CUDA(cudaGetLastError());
@@ -366,9 +670,9 @@ int matrix_spmv(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) 
     }
     m->ctx->launches += 2;
     switch (m->value_type) {
-        case FD2_VALUES_F16: return launch_spmv<__half>(m, x, y, st);
-        case FD2_VALUES_BF16: return launch_spmv<__nv_bfloat16>(m, x, y, st);
-        default: return launch_spmv<float>(m, x, y, st);
+        case FD2_VALUES_F16: return launch_stream<__half>(m, x, y, st);
+        case FD2_VALUES_BF16: return launch_stream<__nv_bfloat16>(m, x, y, st);
+        default: return launch_stream<float>(m, x, y, st);
     }
 }
 
@@ -379,14 +683,17 @@ using namespace fd2;
 extern "C" {
 
 int fd2_matrix_create(fd2_context* ctx, int64_t rows, int64_t cols, int64_t nnz, const int64_t* h_off,
-                      const int64_t* h_col, const float* h_val, int value_type, fd2_matrix** out) {
+                      const int64_t* h_col, const float* h_val, int value_type, int index_format,
+                      fd2_matrix** out) {
     FD2_REQUIRE(ctx && h_off && out && (nnz == 0 || (h_col && h_val)), FD2_ERR_INVALID_ARGUMENT,
                 "matrix_create: null argument");
-    FD2_REQUIRE(rows >= 0 && cols >= 0 && nnz >= 0 && cols < ((int64_t)1 << 31), FD2_ERR_INVALID_ARGUMENT,
-                "matrix_create: sizes rows=%lld cols=%lld nnz=%lld", (long long)rows, (long long)cols,
-                (long long)nnz);
+    FD2_REQUIRE(rows >= 0 && rows < ((int64_t)1 << 31) && cols >= 0 && cols < ((int64_t)1 << 31) && nnz >= 0,
+                FD2_ERR_INVALID_ARGUMENT, "matrix_create: sizes rows=%lld cols=%lld nnz=%lld", (long long)rows,
+                (long long)cols, (long long)nnz);
     FD2_REQUIRE(value_type >= FD2_VALUES_F32 && value_type <= FD2_VALUES_BF16, FD2_ERR_INVALID_ARGUMENT,
                 "matrix_create: value type %d", value_type);
+    FD2_REQUIRE(index_format == FD2_INDEX_I32 || index_format == FD2_INDEX_PACKED16, FD2_ERR_INVALID_ARGUMENT,
+                "matrix_create: index format %d", index_format);
     FD2_REQUIRE(h_off[0] == 0 && h_off[rows] == nnz, FD2_ERR_INVALID_ARGUMENT,
                 "matrix_create: offsets must run from 0 to nnz");
     for (int64_t r = 0; r < rows; r++)
@@ -404,6 +711,7 @@ int fd2_matrix_create(fd2_context* ctx, int64_t rows, int64_t cols, int64_t nnz,
     m->cols = cols;
     m->nnz = nnz;
     m->value_type = value_type;
+    m->index_format = index_format;
     m->scale_axis = value_type == FD2_VALUES_F32 ? FD2_SCALE_NONE : FD2_SCALE_COLS;
     cudaStream_t st = ctx->stream;
     float* d_f = nullptr;
@@ -415,7 +723,7 @@ int fd2_matrix_create(fd2_context* ctx, int64_t rows, int64_t cols, int64_t nnz,
         delete m;
         return rc;
     };
-    int rc = matrix_alloc(m);
+    int rc = matrix_alloc(m, st);
     if (rc) return fail(rc);
     cudaError_t e = cudaMemcpyAsync(m->d_off, h_off, (rows + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess && nnz)
@@ -442,17 +750,13 @@ int fd2_matrix_create(fd2_context* ctx, int64_t rows, int64_t cols, int64_t nnz,
         }
         if (e == cudaSuccess) e = cudaGetLastError();
     }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host staging buffers must outlive the copies
     if (e != cudaSuccess) {
         set_error("matrix_create: %s", cudaGetErrorString(e));
         return fail(e == cudaErrorMemoryAllocation ? FD2_ERR_OUT_OF_MEMORY : FD2_ERR_CUDA);
     }
-    rc = matrix_plan(m, st);
+    rc = matrix_finalize(m, st);
     if (rc) return fail(rc);
-    e = cudaStreamSynchronize(st);  // the host staging buffers must outlive the copies
-    if (e != cudaSuccess) {
-        set_error("matrix_create: %s", cudaGetErrorString(e));
-        return fail(FD2_ERR_CUDA);
-    }
     if (d_f) cudaFree(d_f);
     if (d_mx) cudaFree(d_mx);
     *out = m;
@@ -473,9 +777,15 @@ int fd2_matrix_info(const fd2_matrix* m, fd2_matrix_info_t* info) {
     info->nnz = m->nnz;
     info->value_type = m->value_type;
     info->scale_axis = m->scale_axis;
+    info->index_format = m->index_format;
+    info->reserved = 0;
+    info->exception_chunks = m->n_exc;
+    const int64_t pad = m->n_chunks * kChunk;
     const int64_t ns = m->scale_axis == FD2_SCALE_ROWS ? m->rows : m->scale_axis == FD2_SCALE_COLS ? m->cols : 0;
-    info->device_bytes =
-        (m->rows + 1) * 8 + m->nnz * (4 + (int64_t)value_size(m->value_type)) + ns * (int64_t)sizeof(float);
+    const int64_t col_bytes =
+        m->index_format == FD2_INDEX_PACKED16 ? pad * 2 + m->n_chunks * 4 + m->n_exc * kChunk * 4 : pad * 4;
+    info->device_bytes = pad * (int64_t)value_size(m->value_type) + col_bytes + pad / 8 + m->n_chunks * 4 +
+                         m->n_nzrows * 4 + ns * (int64_t)sizeof(float);
     return FD2_OK;
 }
 
@@ -485,29 +795,34 @@ int fd2_matrix_to_host(const fd2_matrix* m, int64_t* h_off, int32_t* h_col, floa
     cudaStream_t st = m->ctx->stream;
     FD2_CHECK_CUDA(cudaMemcpyAsync(h_off, m->d_off, (m->rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, st));
     if (m->nnz) {
-        FD2_CHECK_CUDA(cudaMemcpyAsync(h_col, m->d_col, m->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
         float* d_f = nullptr;
-        FD2_CHECK_CUDA(cudaMalloc(&d_f, m->nnz * sizeof(float)));
-        switch (m->value_type) {
-            case FD2_VALUES_F16:
-                dequantize<__half><<<grid_for(m->nnz), 256, 0, st>>>(m->d_off, m->rows, m->d_col,
-                                                                     (const __half*)m->d_val, m->d_scale,
-                                                                     m->scale_axis, m->nnz, d_f);
-                break;
-            case FD2_VALUES_BF16:
-                dequantize<__nv_bfloat16><<<grid_for(m->nnz), 256, 0, st>>>(
-                    m->d_off, m->rows, m->d_col, (const __nv_bfloat16*)m->d_val, m->d_scale, m->scale_axis, m->nnz,
-                    d_f);
-                break;
-            default:
-                dequantize<float><<<grid_for(m->nnz), 256, 0, st>>>(m->d_off, m->rows, m->d_col,
-                                                                    (const float*)m->d_val, m->d_scale,
-                                                                    m->scale_axis, m->nnz, d_f);
+        int32_t* d_c = nullptr;
+        cudaError_t e = cudaMalloc(&d_f, m->nnz * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc(&d_c, m->nnz * sizeof(int32_t));
+        if (e == cudaSuccess) {
+            switch (m->value_type) {
+                case FD2_VALUES_F16:
+                    unpack_entries<__half><<<grid_for(m->nnz), 256, 0, st>>>(
+                        m->d_off, m->rows, m->cols_view(), (const __half*)m->d_val, m->d_scale, m->scale_axis, m->nnz,
+                        d_c, d_f);
+                    break;
+                case FD2_VALUES_BF16:
+                    unpack_entries<__nv_bfloat16><<<grid_for(m->nnz), 256, 0, st>>>(
+                        m->d_off, m->rows, m->cols_view(), (const __nv_bfloat16*)m->d_val, m->d_scale, m->scale_axis,
+                        m->nnz, d_c, d_f);
+                    break;
+                default:
+                    unpack_entries<float><<<grid_for(m->nnz), 256, 0, st>>>(m->d_off, m->rows, m->cols_view(),
+                                                                            (const float*)m->d_val, m->d_scale,
+                                                                            m->scale_axis, m->nnz, d_c, d_f);
+            }
+            e = cudaGetLastError();
         }
-        cudaError_t e = cudaGetLastError();
         if (e == cudaSuccess) e = cudaMemcpyAsync(h_val, d_f, m->nnz * sizeof(float), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_col, d_c, m->nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        cudaFree(d_f);
+        if (d_f) cudaFree(d_f);
+        if (d_c) cudaFree(d_c);
         FD2_CHECK_CUDA(e);
     }
     FD2_CHECK_CUDA(cudaStreamSynchronize(st));
@@ -516,19 +831,24 @@ int fd2_matrix_to_host(const fd2_matrix* m, int64_t* h_off, int32_t* h_col, floa
 
 int fd2_matrix_transpose(const fd2_matrix* m, fd2_matrix** out) {
     FD2_REQUIRE(m && out, FD2_ERR_INVALID_ARGUMENT, "matrix_transpose: null argument");
-    FD2_REQUIRE(m->rows < ((int64_t)1 << 31), FD2_ERR_INVALID_ARGUMENT,
-                "matrix_transpose: %lld rows do not fit int32 columns", (long long)m->rows);
+    return matrix_transpose_fmt(m, m->index_format, out);
+}
+
+}  // extern "C"
+
+int fd2::matrix_transpose_fmt(const fd2_matrix* m, int index_format, fd2_matrix** out) {
     auto* t = new fd2_matrix();
     t->ctx = m->ctx;
     t->rows = m->cols;
     t->cols = m->rows;
     t->nnz = m->nnz;
     t->value_type = m->value_type;
+    t->index_format = index_format;
     t->scale_axis = m->scale_axis == FD2_SCALE_ROWS   ? FD2_SCALE_COLS
                     : m->scale_axis == FD2_SCALE_COLS ? FD2_SCALE_ROWS
                                                       : FD2_SCALE_NONE;
     cudaStream_t st = m->ctx->stream;
-    int rc = matrix_alloc(t);
+    int rc = matrix_alloc(t, st);
     if (rc == FD2_OK && t->d_scale) {
         const int64_t ns = t->scale_axis == FD2_SCALE_ROWS ? t->rows : t->cols;
         if (ns && cudaMemcpyAsync(t->d_scale, m->d_scale, ns * sizeof(float), cudaMemcpyDeviceToDevice, st) !=
@@ -547,8 +867,7 @@ int fd2_matrix_transpose(const fd2_matrix* m, fd2_matrix** out) {
             }
         }
     }
-    if (rc == FD2_OK) rc = matrix_plan(t, st);
-    if (rc == FD2_OK && cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    if (rc == FD2_OK) rc = matrix_finalize(t, st);
     if (rc) {
         matrix_free(t);
         delete t;
@@ -558,9 +877,7 @@ int fd2_matrix_transpose(const fd2_matrix* m, fd2_matrix** out) {
     return FD2_OK;
 }
 
-int fd2_matrix_spmv(const fd2_matrix* m, const float* d_x, float* d_y, void* stream) {
+extern "C" int fd2_matrix_spmv(const fd2_matrix* m, const float* d_x, float* d_y, void* stream) {
     FD2_REQUIRE(m && d_y && (m->cols == 0 || d_x), FD2_ERR_INVALID_ARGUMENT, "matrix_spmv: null argument");
     return matrix_spmv(m, d_x, d_y, (cudaStream_t)stream);
 }
-
-}  // extern "C"

@@ -318,10 +318,12 @@ using namespace fd2;
 extern "C" {
 
 int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, int64_t n_voxels, int64_t n_voi,
-                     int value_type, fd2_matrix** A, fd2_matrix** AT) {
+                     int value_type, int index_format, fd2_matrix** A, fd2_matrix** AT) {
     FD2_REQUIRE(dose && h_voxel_row && A && AT, FD2_ERR_INVALID_ARGUMENT, "voi_matrices: null argument");
     FD2_REQUIRE(value_type >= FD2_VALUES_F32 && value_type <= FD2_VALUES_BF16, FD2_ERR_INVALID_ARGUMENT,
                 "voi_matrices: value type %d", value_type);
+    FD2_REQUIRE(index_format == FD2_INDEX_I32 || index_format == FD2_INDEX_PACKED16, FD2_ERR_INVALID_ARGUMENT,
+                "voi_matrices: index format %d", index_format);
     fd2_csr_info_t info;
     FD2_TRY(fd2_csr_ensemble_info(dose, &info));
     FD2_REQUIRE((int64_t)info.n_cols == n_voxels, FD2_ERR_INVALID_ARGUMENT,
@@ -388,13 +390,10 @@ int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, i
     int rc = offsets_from_counts(d_count, rows, t->d_off, &nnz, st);
     if (rc) return fail(rc);
     t->nnz = nnz;
-    if (cudaMalloc(&t->d_col, std::max<int64_t>(nnz, 1) * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&t->d_val, std::max<int64_t>(nnz, 1) * value_size(value_type)) != cudaSuccess)
-        return fail(FD2_ERR_OUT_OF_MEMORY);
+    rc = matrix_alloc_entries(t, st);
+    if (rc) return fail(rc);
     const float* dst_scale = nullptr;
     if (t->scale_axis == FD2_SCALE_ROWS) {
-        if (cudaMalloc(&t->d_scale, std::max<int64_t>(rows, 1) * sizeof(float)) != cudaSuccess)
-            return fail(FD2_ERR_OUT_OF_MEMORY);
         if (d_src_scale && rows)  // a 16-bit source keeps its per-beamlet scale
             cudaMemcpyAsync(t->d_scale, d_src_scale, rows * sizeof(float), cudaMemcpyDeviceToDevice, st);
         else
@@ -418,11 +417,13 @@ int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, i
         if (cudaGetLastError() != cudaSuccess) return fail(FD2_ERR_CUDA);
     }
     if (cudaStreamSynchronize(st) != cudaSuccess) return fail(FD2_ERR_CUDA);
+    rc = matrix_finalize(t, st);  // storage order, which the transpose reads
+    if (rc) return fail(rc);
     fd2_matrix *a = nullptr, *at = nullptr;
-    rc = fd2_matrix_transpose(t, &a);  // VOI rows, beamlet columns ascending
+    rc = matrix_transpose_fmt(t, index_format, &a);  // VOI rows, beamlet columns ascending
     drop();
     if (rc) return rc;
-    rc = fd2_matrix_transpose(a, &at);  // beamlet rows, VOI columns ascending
+    rc = matrix_transpose_fmt(a, index_format, &at);  // beamlet rows, VOI columns ascending
     if (rc) {
         fd2_matrix_destroy(a);
         return rc;
@@ -433,8 +434,10 @@ int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, i
 }
 
 int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t window, float density, uint64_t seed,
-                         int value_type, fd2_matrix** A, fd2_matrix** AT) {
+                         int value_type, int index_format, fd2_matrix** A, fd2_matrix** AT) {
     FD2_REQUIRE(ctx && A && AT, FD2_ERR_INVALID_ARGUMENT, "matrix_synthetic: null argument");
+    FD2_REQUIRE(index_format == FD2_INDEX_I32 || index_format == FD2_INDEX_PACKED16, FD2_ERR_INVALID_ARGUMENT,
+                "matrix_synthetic: index format %d", index_format);
     FD2_REQUIRE(rows > 0 && cols > 0 && rows < ((int64_t)1 << 31) && cols < ((int64_t)1 << 31) && window > 0 &&
                     density > 0.0f && density <= 1.0f,
                 FD2_ERR_INVALID_ARGUMENT, "matrix_synthetic: rows %lld cols %lld window %lld density %g",
@@ -458,6 +461,7 @@ int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t w
         m[i]->rows = i == 0 ? rows : cols;
         m[i]->cols = i == 0 ? cols : rows;
         m[i]->scale_axis = !half ? FD2_SCALE_NONE : i == 0 ? FD2_SCALE_COLS : FD2_SCALE_ROWS;
+        m[i]->index_format = index_format;
     }
     Guard g;
     int64_t* d_count = nullptr;
@@ -474,13 +478,9 @@ int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t w
     int rc = offsets_from_counts(d_count, cols, t->d_off, &nnz, st);
     if (rc) return fail(rc);
     t->nnz = nnz;
-    if (cudaMalloc(&t->d_col, std::max<int64_t>(nnz, 1) * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&t->d_val, std::max<int64_t>(nnz, 1) * value_size(value_type)) != cudaSuccess)
-        return fail(FD2_ERR_OUT_OF_MEMORY);
-    if (half) {
-        if (cudaMalloc(&t->d_scale, cols * sizeof(float)) != cudaSuccess) return fail(FD2_ERR_OUT_OF_MEMORY);
-        unit_or_max<<<blocks_for(cols), 256, 0, st>>>(d_max, t->d_scale, cols);
-    }
+    rc = matrix_alloc_entries(t, st);
+    if (rc) return fail(rc);
+    if (half) unit_or_max<<<blocks_for(cols), 256, 0, st>>>(d_max, t->d_scale, cols);
     switch (value_type) {
         case FD2_VALUES_F16:
             synth_t_fill<__half><<<(unsigned)cols, kThreads, 0, st>>>(sp, t->d_scale, t->d_off, t->d_col,
@@ -509,13 +509,9 @@ int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t w
         return fail(FD2_ERR_CUDA);
     }
     a->nnz = nnz;
-    if (cudaMalloc(&a->d_col, std::max<int64_t>(nnz, 1) * sizeof(int32_t)) != cudaSuccess ||
-        cudaMalloc(&a->d_val, std::max<int64_t>(nnz, 1) * value_size(value_type)) != cudaSuccess)
-        return fail(FD2_ERR_OUT_OF_MEMORY);
-    if (half) {
-        if (cudaMalloc(&a->d_scale, cols * sizeof(float)) != cudaSuccess) return fail(FD2_ERR_OUT_OF_MEMORY);
-        cudaMemcpyAsync(a->d_scale, t->d_scale, cols * sizeof(float), cudaMemcpyDeviceToDevice, st);
-    }
+    rc = matrix_alloc_entries(a, st);
+    if (rc) return fail(rc);
+    if (half) cudaMemcpyAsync(a->d_scale, t->d_scale, cols * sizeof(float), cudaMemcpyDeviceToDevice, st);
     switch (value_type) {
         case FD2_VALUES_F16:
             synth_fill<__half><<<wblocks, 256, 0, st>>>(sp, a->d_scale, a->d_off, a->d_col, (__half*)a->d_val);
@@ -528,8 +524,9 @@ int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t w
             synth_fill<float><<<wblocks, 256, 0, st>>>(sp, nullptr, a->d_off, a->d_col, (float*)a->d_val);
     }
     if (cudaGetLastError() != cudaSuccess) return fail(FD2_ERR_CUDA);
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fail(FD2_ERR_CUDA);
     for (auto* q : m) {
-        rc = matrix_plan(q, st);
+        rc = matrix_finalize(q, st);
         if (rc) return fail(rc);
     }
     if (cudaStreamSynchronize(st) != cudaSuccess) return fail(FD2_ERR_CUDA);

@@ -17,11 +17,13 @@ from . import _lib
 from .api import VALUE_TYPES, _p, _stream_ptr, _torch
 
 SCALE_AXES = {0: "none", 1: "rows", 2: "cols"}
+INDEX_FORMATS = {"i32": 0, "packed16": 1}
 
 
 class _MatInfo(C.Structure):
     _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("nnz", C.c_int64), ("value_type", C.c_int32),
-                ("scale_axis", C.c_int32), ("device_bytes", C.c_int64)]
+                ("scale_axis", C.c_int32), ("device_bytes", C.c_int64), ("index_format", C.c_int32),
+                ("reserved", C.c_int32), ("exception_chunks", C.c_int64)]
 
 
 class _State(C.Structure):
@@ -57,37 +59,41 @@ class Matrix:
         self.h = handle
 
     @classmethod
-    def from_csr(cls, ctx, offsets, columns, values, n_cols, value_type="f32"):
+    def from_csr(cls, ctx, offsets, columns, values, n_cols, value_type="f32", index_format="i32"):
         off = np.ascontiguousarray(offsets, np.int64)
         col = np.ascontiguousarray(columns, np.int64)
         val = np.ascontiguousarray(values, np.float32)
         h = C.c_void_p()
         _lib.check(ctx.lib.fd2_matrix_create(ctx.h, len(off) - 1, int(n_cols), len(col), _p(off), _p(col), _p(val),
-                                             VALUE_TYPES[value_type], C.byref(h)), "matrix_create")
+                                             VALUE_TYPES[value_type], INDEX_FORMATS[index_format], C.byref(h)),
+                   "matrix_create")
         return cls(ctx, h)
 
     @classmethod
-    def synthetic(cls, ctx, rows, cols, window, density, seed=1, value_type="f32"):
+    def synthetic(cls, ctx, rows, cols, window, density, seed=1, value_type="f32", index_format="i32"):
         """Seeded synthetic VOI pair (A, AT) built on the device."""
         a, at = C.c_void_p(), C.c_void_p()
         _lib.check(ctx.lib.fd2_matrix_synthetic(ctx.h, rows, cols, window, density, seed, VALUE_TYPES[value_type],
-                                                C.byref(a), C.byref(at)), "matrix_synthetic")
+                                                INDEX_FORMATS[index_format], C.byref(a), C.byref(at)),
+                   "matrix_synthetic")
         return cls(ctx, a), cls(ctx, at)
 
     @classmethod
-    def voi(cls, ctx, ensemble, voxel_row, n_voi, value_type="f32"):
+    def voi(cls, ctx, ensemble, voxel_row, n_voi, value_type="f32", index_format="i32"):
         """getStructFilter + parallelSpGEMM: (A, AT) of the VOI rows of a dose matrix."""
         vr = np.ascontiguousarray(voxel_row, np.int32)
         a, at = C.c_void_p(), C.c_void_p()
         _lib.check(ctx.lib.fd2_voi_matrices(ensemble.h, _p(vr), vr.size, int(n_voi), VALUE_TYPES[value_type],
-                                            C.byref(a), C.byref(at)), "voi_matrices")
+                                            INDEX_FORMATS[index_format], C.byref(a), C.byref(at)), "voi_matrices")
         return cls(ctx, a), cls(ctx, at)
 
     def info(self):
         i = _MatInfo()
         _lib.check(self.ctx.lib.fd2_matrix_info(self.h, C.byref(i)), "matrix_info")
+        fmt = {v: k for k, v in INDEX_FORMATS.items()}[i.index_format]
         return dict(rows=i.rows, cols=i.cols, nnz=i.nnz, value_type=i.value_type,
-                    scale_axis=SCALE_AXES[i.scale_axis], device_bytes=i.device_bytes)
+                    scale_axis=SCALE_AXES[i.scale_axis], device_bytes=i.device_bytes, index_format=fmt,
+                    exception_chunks=i.exception_chunks)
 
     @property
     def shape(self):

@@ -50,11 +50,27 @@ typedef enum fd2_scale_axis {
     FD2_SCALE_COLS = 2
 } fd2_scale_axis;
 
+/*
+ * Column index storage.  I32: one int32 per nonzero.  PACKED16: the nonzeros
+ * are cut into chunks of 256; each chunk stores one int32 base column and a
+ * 16-bit offset per nonzero, and a chunk whose columns span 65536 or more
+ * keeps int32 columns in a side array -- 2 bytes per nonzero plus 4 per chunk
+ * for matrices whose rows have local column ranges (VOI matrices, and any
+ * matrix with at most 65536 columns).
+ */
+typedef enum fd2_index_format {
+    FD2_INDEX_I32 = 0,
+    FD2_INDEX_PACKED16 = 1
+} fd2_index_format;
+
 typedef struct fd2_matrix_info {
     int64_t rows, cols, nnz;
     int32_t value_type;   /* fd2_value_type */
     int32_t scale_axis;   /* fd2_scale_axis */
-    int64_t device_bytes; /* offsets + columns + values + scales */
+    int64_t device_bytes; /* bytes one SpMV pass streams: offsets/plan, columns, values, scales */
+    int32_t index_format; /* fd2_index_format */
+    int32_t reserved;
+    int64_t exception_chunks; /* PACKED16 chunks stored with int32 columns */
 } fd2_matrix_info_t;
 
 /*
@@ -63,7 +79,8 @@ typedef struct fd2_matrix_info {
  * value types are scaled per column (column max -> 1) before rounding.
  */
 int fd2_matrix_create(fd2_context* ctx, int64_t rows, int64_t cols, int64_t nnz, const int64_t* h_offsets,
-                      const int64_t* h_columns, const float* h_values, int value_type, fd2_matrix** out);
+                      const int64_t* h_columns, const float* h_values, int value_type, int index_format,
+                      fd2_matrix** out);
 int fd2_matrix_destroy(fd2_matrix* m);
 int fd2_matrix_info(const fd2_matrix* m, fd2_matrix_info_t* info);
 /* Copy to host as FP32 (scales applied): offsets [rows+1], columns [nnz], values [nnz]. */
@@ -86,7 +103,7 @@ int fd2_matrix_spmv(const fd2_matrix* m, const float* d_x, float* d_y, void* str
  * n_voxels must equal the dose matrix's column count.
  */
 int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, int64_t n_voxels, int64_t n_voi,
-                     int value_type, fd2_matrix** A, fd2_matrix** AT);
+                     int value_type, int index_format, fd2_matrix** A, fd2_matrix** AT);
 
 /*
  * Seeded synthetic VOI matrix pair for optimizer benchmarks: rows x cols with
@@ -98,7 +115,7 @@ int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, i
  * values.
  */
 int fd2_matrix_synthetic(fd2_context* ctx, int64_t rows, int64_t cols, int64_t window, float density, uint64_t seed,
-                         int value_type, fd2_matrix** A, fd2_matrix** AT);
+                         int value_type, int index_format, fd2_matrix** A, fd2_matrix** AT);
 
 /*
  * fluenceGradInit for one beam (IMRTOpt/src/IMRTOptimize_var.cpp:59-180 with

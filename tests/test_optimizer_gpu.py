@@ -41,14 +41,16 @@ def _dense(m, rows):
     return d
 
 
+@pytest.mark.parametrize("fmt", ["i32", "packed16"])
 @pytest.mark.parametrize("vt", ["f32", "f16", "bf16"])
-def test_spmv_matches_exact_product(ctx, vt):
+def test_spmv_matches_exact_product(ctx, vt, fmt):
     import torch
 
     rng = np.random.default_rng(3)
-    rows, cols = 700, 6000  # rows 3 and 400 span several 2048-item tiles
+    rows, cols = 700, 6000  # rows 3 and 400 span many 256-nonzero chunks and several warps
     m = _random_csr(rng, rows, cols, 0.01, long_rows=(3, 400))
-    M = optimize.Matrix.from_csr(ctx, *m[:3], cols, value_type=vt)
+    M = optimize.Matrix.from_csr(ctx, *m[:3], cols, value_type=vt, index_format=fmt)
+    assert M.info()["index_format"] == fmt
     off, col, val = M.to_host()  # the stored (rounded) values, scale applied
     np.testing.assert_array_equal(off, m[0])
     np.testing.assert_array_equal(col, m[1])
@@ -67,6 +69,55 @@ def test_spmv_matches_exact_product(ctx, vt):
     np.testing.assert_array_equal(y, y2)
 
 
+@pytest.mark.parametrize("vt,fmt", [("f32", "i32"), ("f16", "packed16")])
+def test_spmv_at_scale_matches_cusparse_and_its_adjoint(ctx, vt, fmt):
+    """400k VOI rows x 4000 beamlets, 3.2e7 nonzeros: A x against cuSPARSE
+    (through torch) on the same stored values, and <A x, y> = <x, A^T y> with
+    A^T generated independently."""
+    import torch
+
+    rows, cols = 400_000, 4000
+    A, AT = optimize.Matrix.synthetic(ctx, rows, cols, rows // 25, 0.5, seed=5, value_type=vt, index_format=fmt)
+    g = torch.Generator(device="cuda").manual_seed(1)
+    x = torch.rand(cols, device="cuda", generator=g)
+    y = torch.rand(rows, device="cuda", generator=g)
+    Ax, ATy = A.spmv(x), AT.spmv(y)
+    torch.cuda.synchronize()
+    lhs = torch.dot(Ax.double(), y.double()).item()
+    rhs = torch.dot(x.double(), ATy.double()).item()
+    assert abs(lhs - rhs) <= 1e-6 * abs(lhs)
+    off, col, val = A.to_host()
+    S = torch.sparse_csr_tensor(torch.from_numpy(off).cuda(), torch.from_numpy(col.astype(np.int64)).cuda(),
+                                torch.from_numpy(val).cuda(), size=(rows, cols))
+    ref = (S @ x.unsqueeze(1)).squeeze(1)
+    bound = (torch.sparse_csr_tensor(S.crow_indices(), S.col_indices(), S.values().abs(), size=(rows, cols))
+             @ x.abs().unsqueeze(1)).squeeze(1)
+    assert torch.all((Ax - ref).abs() <= 2e-5 * bound + 1e-30)
+
+
+def test_packed_columns_with_wide_chunks(ctx):
+    """Columns spread over 300k: most chunks span more than 65536 columns and
+    keep int32 columns; short rows (many row starts per chunk) and empty rows."""
+    import torch
+
+    rng = np.random.default_rng(8)
+    rows, cols = 4000, 300_000
+    m = _random_csr(rng, rows, cols, 2e-4, long_rows=(17,), empty_frac=0.3)
+    ref = optimize.Matrix.from_csr(ctx, *m[:3], cols, value_type="f32", index_format="i32")
+    M = optimize.Matrix.from_csr(ctx, *m[:3], cols, value_type="f32", index_format="packed16")
+    info = M.info()
+    assert 0 < info["exception_chunks"] < (m[0][-1] + 255) // 256
+    for a, b in zip(M.to_host(), ref.to_host()):
+        np.testing.assert_array_equal(a, b)
+    x = torch.from_numpy(rng.standard_normal(cols).astype(np.float32)).cuda()
+    np.testing.assert_array_equal(M.spmv(x).cpu().numpy(), ref.spmv(x).cpu().numpy())
+    # its transpose (300k rows, columns < 4000) packs without exceptions
+    T = M.transpose()
+    assert T.info()["index_format"] == "packed16" and T.info()["exception_chunks"] == 0
+    for a, b in zip(T.to_host(), ref.transpose().to_host()):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_transpose_is_exact(ctx):
     rng = np.random.default_rng(4)
     m = _random_csr(rng, 300, 2500, 0.02, long_rows=(7,))
@@ -83,9 +134,10 @@ def test_transpose_is_exact(ctx):
         np.testing.assert_array_equal(t_val, r_val)
 
 
-def test_synthetic_pair_is_an_exact_transpose(ctx):
+@pytest.mark.parametrize("fmt", ["i32", "packed16"])
+def test_synthetic_pair_is_an_exact_transpose(ctx, fmt):
     for vt in ("f32", "f16"):
-        A, AT = optimize.Matrix.synthetic(ctx, 6000, 300, 900, 0.3, seed=7, value_type=vt)
+        A, AT = optimize.Matrix.synthetic(ctx, 6000, 300, 900, 0.3, seed=7, value_type=vt, index_format=fmt)
         ia, it = A.info(), AT.info()
         assert ia["nnz"] == it["nnz"] > 0 and (ia["rows"], ia["cols"]) == (it["cols"], it["rows"])
         T = A.transpose()
@@ -112,8 +164,8 @@ def _problem_case(seed=11, n_beams=6, fd=8, per_beam=40, n_ptv=500, n_oar=1500):
     return A, D, w, groups, n_ptv, n_oar, n
 
 
-def _gpu_problem(ctx, A, D, w, n_ptv, n_oar, n, vt="f32", gamma=1.0, eta=0.1):
-    Am = optimize.Matrix.from_csr(ctx, *A[:3], n, value_type=vt)
+def _gpu_problem(ctx, A, D, w, n_ptv, n_oar, n, vt="f32", gamma=1.0, eta=0.1, fmt="i32"):
+    Am = optimize.Matrix.from_csr(ctx, *A[:3], n, value_type=vt, index_format=fmt)
     ATm = Am.transpose()
     Dm = optimize.Matrix.from_csr(ctx, *D[:3], n)
     DTm = Dm.transpose()
@@ -198,15 +250,17 @@ def test_half_precision_objective_within_a_tenth_percent(ctx):
     A, D, w, groups, n_ptv, n_oar, n = _problem_case(seed=13)
     x0 = np.random.default_rng(2).random(n).astype(np.float32) * 0.02
     res = {}
-    for vt in ("f32", "f16", "bf16"):
-        P = _gpu_problem(ctx, A, D, w, n_ptv, n_oar, n, vt=vt)
-        res[vt] = P.polish(x0, step_size=1e-3, iters=100)["loss"][-1]
-    assert abs(res["f16"] - res["f32"]) <= 1e-3 * abs(res["f32"])
-    assert abs(res["bf16"] - res["f32"]) <= 1e-2 * abs(res["f32"])
+    for vt, fmt in (("f32", "i32"), ("f32", "packed16"), ("f16", "packed16"), ("bf16", "packed16")):
+        P = _gpu_problem(ctx, A, D, w, n_ptv, n_oar, n, vt=vt, fmt=fmt)
+        res[vt, fmt] = P.polish(x0, step_size=1e-3, iters=100)["loss"][-1]
+    f32 = res["f32", "i32"]
+    assert abs(res["f32", "packed16"] - f32) <= 1e-6 * abs(f32)  # same values, same order per row
+    assert abs(res["f16", "packed16"] - f32) <= 1e-3 * abs(f32)
+    assert abs(res["bf16", "packed16"] - f32) <= 1e-2 * abs(f32)
 
 
-@pytest.mark.parametrize("vt", ["f32", "f16"])
-def test_voi_restriction_of_a_dose_matrix(ctx, vt):
+@pytest.mark.parametrize("vt,fmt", [("f32", "i32"), ("f16", "packed16")])
+def test_voi_restriction_of_a_dose_matrix(ctx, vt, fmt):
     case = small_case()
     ph = case["phantom"]
     dens, sp, kn = api.Density(ctx, ph.density, ph.volume), api.Spectrum(ctx, case["spectrum"]), \
@@ -221,7 +275,7 @@ def test_voi_restriction_of_a_dose_matrix(ctx, vt):
     voxel_row[ptv] = np.arange(len(ptv))
     voxel_row[oar] = len(ptv) + np.arange(len(oar))
     n_voi = len(ptv) + len(oar)
-    A, AT = optimize.Matrix.voi(ctx, ens, voxel_row, n_voi, value_type=vt)
+    A, AT = optimize.Matrix.voi(ctx, ens, voxel_row, n_voi, value_type=vt, index_format=fmt)
     assert A.shape == (n_voi, len(ro) - 1)
     # exact restriction on the host: keep, renumber, transpose
     rows = np.repeat(np.arange(len(ro) - 1), np.diff(ro))
