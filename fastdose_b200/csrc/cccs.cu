@@ -41,6 +41,9 @@ namespace fd2 {
 namespace {
 
 constexpr int kStepCap = 1 << 20;  // per-slice step cap (the watchdog bound)
+// The 16x16 march is compiled for at most 8 azimuth warps (register budget
+// for 4 such blocks of 256 threads, i.e. 5 blocks of 192 threads, per SM).
+constexpr int kFx16Threads = 256;
 
 struct RayGeom {  // per-beamlet scalars the march needs
     float hx, hy;      // fmap_size / 2
@@ -105,7 +108,7 @@ __device__ __forceinline__ bool crosses16(float b, float n) {
 // the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
 // sums).  RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
 template <int RPL, bool kFx16>
-__global__ void __launch_bounds__(768) cccs_kernel(const fd2_beam_t* __restrict__ beams,
+__global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
                                                    float* const* __restrict__ dose,
@@ -197,13 +200,20 @@ __global__ void __launch_bounds__(768) cccs_kernel(const fd2_beam_t* __restrict_
                     const bool wrapx = crosses16(btx, ntx);
                     const float dxp = (ntx - 8.0f) * g.bsx * fe - (btx - 8.0f) * g.bsx * fs;
                     const float dxz2 = dxp * dxp + dzp * dzp;
+                    // The y half depends only on the ray's row offset (16 values per
+                    // step): lane l computes it for row (l & 15), and each ray takes
+                    // its row's result by shuffle -- the same operations on the same
+                    // inputs as a per-ray evaluation, done once instead of 16 times.
+                    const float bty = __fadd_rn(c.y, lx), nty = __fadd_rn(np.y, lx);
+                    const int ycode = mid_index16(bty, nty) | (crosses16(bty, nty) ? 16 : 0);
+                    const float dyq = (nty - 8.0f) * g.bsy * fe - (bty - 8.0f) * g.bsy * fs;
 #pragma unroll
                     for (int j = 0; j < RPL; j++) {
-                        const float ly = (float)((lane >> 4) + 2 * j);
-                        const float bty = __fadd_rn(c.y, ly), nty = __fadd_rn(np.y, ly);
-                        const int mi = cx + 16 * mid_index16(bty, nty);
-                        const bool wrap = wrapx || crosses16(bty, nty);
-                        const float dyp = (nty - 8.0f) * g.bsy * fe - (bty - 8.0f) * g.bsy * fs;
+                        const int row = (lane >> 4) + 2 * j;
+                        const int yc = __shfl_sync(0xffffffffu, ycode, row);
+                        const float dyp = __shfl_sync(0xffffffffu, dyq, row);
+                        const int mi = cx + 16 * (yc & 15);
+                        const bool wrap = wrapx || (yc & 16);
                         const float l2 = dxz2 + dyp * dyp;
                         const float len = l2 * rsqrtf(l2);
                         const float2 trv = tr[mi];
@@ -346,6 +356,7 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     const unsigned blocks = (unsigned)(schedule == 1 ? n_beams * fwd.size() : n_beams);
     bool all16 = true;
     for (size_t i = 0; i < n_beams && all16; i++) all16 = h_beams[i].fmap_size[0] == 16 && h_beams[i].fmap_size[1] == 16;
+    all16 = all16 && threads <= kFx16Threads;
     if (all16) {
         FD2_CHECK_CUDA(
             cudaFuncSetAttribute(cccs_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
@@ -551,7 +562,7 @@ extern "C" int fd2_dose_compute_static(size_t fmap_npixels, size_t n_beams, cons
     const unsigned blocks = (unsigned)n_beams;
     const float* const* T = (const float* const*)d_terma;
     const float* const* R = (const float* const*)d_density_bev;
-    if (all16) {
+    if (all16 && threads <= kFx16Threads) {
         FD2_CHECK_CUDA(
             cudaFuncSetAttribute(cccs_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
         cccs_kernel<8, true><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0, d_status);

@@ -151,17 +151,51 @@ constexpr int kColThreads = 256;
 constexpr int kPerThread = 4;
 constexpr int kColChunk = kColThreads * kPerThread;
 
+// Voxels of the row (y, z) of a beamlet's box that can be candidates: the
+// candidate test requires the voxel centre within r0 = hdiag + extent + slack
+// of the beamlet axis, and along a row the squared distance to the axis is a
+// quadratic in x, so the admissible x form one interval.  It is solved in
+// double and widened by one voxel on each side, so it contains every x the
+// float test accepts; the exact test still runs on each voxel of it.
+__device__ __forceinline__ void row_interval(const ColumnInfo& ci, int y, int z, float3 vs, float r0, int& xa,
+                                             int& xb) {
+    const double cx0 = 0.5 * vs.x - ci.src[0], cy = (y + 0.5) * vs.y - ci.src[1], cz = (z + 0.5) * vs.z - ci.src[2];
+    const double A0 = ci.R[0] * cx0 + ci.R[1] * cy + ci.R[2] * cz, A1 = (double)ci.R[0] * vs.x;
+    const double C0 = ci.R[6] * cx0 + ci.R[7] * cy + ci.R[8] * cz, C1 = (double)ci.R[6] * vs.x;
+    const double a = A1 * A1 + C1 * C1, b = A0 * A1 + C0 * C1, c = A0 * A0 + C0 * C0 - (double)r0 * r0;
+    xa = ci.box[0];
+    xb = ci.box[3];
+    if (a < 1e-12) {  // row parallel to the beamlet axis
+        if (c > 1e-6 * r0 * r0) xb = xa;
+        return;
+    }
+    const double disc = b * b - a * c;
+    if (disc < 0.0) {
+        xb = xa;
+        return;
+    }
+    const double s = sqrt(disc);
+    const double lo = (-b - s) / a, hi = (-b + s) / a;
+    xa = max(xa, (int)floor(lo) - 1);
+    xb = min(xb, (int)ceil(hi) + 2);
+    if (xb < xa) xb = xa;
+}
+
 // Pass 1: number of candidate voxels of each beamlet (its row capacity).
 __global__ void __launch_bounds__(kColThreads) column_count_kernel(const ColumnInfo* __restrict__ infos,
                                                                   uint32_t* __restrict__ counts, int nx, int ny,
                                                                   float3 vs, float hdiag, float extent) {
     const ColumnInfo ci = infos[blockIdx.x];
-    const int bx = ci.box[3] - ci.box[0], by = ci.box[4] - ci.box[1], bz = ci.box[5] - ci.box[2];
-    const long long n = (long long)bx * by * bz;
+    const int by = ci.box[4] - ci.box[1], bz = ci.box[5] - ci.box[2];
+    const int rows = by * bz;
+    const float r0 = hdiag + extent + 2e-3f;
     uint32_t cnt = 0;
-    for (long long i = threadIdx.x; i < n; i += kColThreads) {
-        int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by), z = ci.box[2] + (int)(i / ((long long)bx * by));
-        cnt += candidate(ci, make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z), hdiag, extent);
+    for (int r = threadIdx.x; r < rows; r += kColThreads) {
+        const int y = ci.box[1] + r % by, z = ci.box[2] + r / by;
+        int xa, xb;
+        row_interval(ci, y, z, vs, r0, xa, xb);
+        for (int x = xa; x < xb; x++)
+            cnt += candidate(ci, make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z), hdiag, extent);
     }
     typedef cub::BlockReduce<uint32_t, kColThreads> Reduce;
     __shared__ typename Reduce::TempStorage tmp;
@@ -172,80 +206,103 @@ __global__ void __launch_bounds__(kColThreads) column_count_kernel(const ColumnI
 
 // Pass 2: values of the candidates, nonzeros compacted in voxel order into
 // the beamlet's temporary segment; writes the row's nnz and max |value|.
+// Rows (y, z) of the box are taken kColThreads at a time in voxel order; their
+// admissible x intervals are concatenated by a scan, and the concatenation is
+// processed kColChunk voxels at a time: candidate test, order-preserving
+// compaction, values, compaction of the nonzeros.
 __global__ void __launch_bounds__(kColThreads) column_value_kernel(
     const ColumnInfo* __restrict__ infos, const float* const* __restrict__ dose, const uint64_t* __restrict__ cap_off,
     int32_t* __restrict__ tmp_col, float* __restrict__ tmp_val, uint32_t* __restrict__ row_nnz,
     float* __restrict__ row_max, int nx, int ny, float3 vs, float hdiag, float extent, int ss) {
     const ColumnInfo ci = infos[blockIdx.x];
     const float* __restrict__ bev = dose[blockIdx.x];
-    const int bx = ci.box[3] - ci.box[0], by = ci.box[4] - ci.box[1], bz = ci.box[5] - ci.box[2];
-    const long long n = (long long)bx * by * bz;
+    const int by = ci.box[4] - ci.box[1], bz = ci.box[5] - ci.box[2];
+    const int rows = by * bz;
+    const float r0 = hdiag + extent + 2e-3f;
     const uint64_t base = cap_off[blockIdx.x];
     const uint64_t cap = cap_off[blockIdx.x + 1] - base;
     typedef cub::BlockScan<uint32_t, kColThreads> Scan;
     typedef cub::BlockReduce<float, kColThreads> RMax;
     __shared__ typename Scan::TempStorage scan_tmp;
     __shared__ typename RMax::TempStorage max_tmp;
-    __shared__ int s_cand[kColChunk];    // box-relative indices of this chunk's candidates, in order
+    __shared__ uint32_t s_roff[kColThreads + 1];  // start of each row's interval in the concatenation
+    __shared__ int s_rx[kColThreads];             // first x of the row's interval
+    __shared__ int s_cand[kColChunk];             // voxel index of this chunk's candidates, in order
     __shared__ float s_val[kColChunk];
     uint32_t written = 0;  // uniform across the block
     float vmax = 0.0f;
-    const long long bxy = (long long)bx * by;
-    for (long long i0 = 0; i0 < n; i0 += kColChunk) {
-        // 1. candidate test, kPerThread consecutive voxels per thread (order-preserving compaction)
-        uint32_t flags = 0, cnt = 0;
+    for (int r0w = 0; r0w < rows; r0w += kColThreads) {
+        const int r = r0w + threadIdx.x;
+        int xa = 0, xb = 0;
+        if (r < rows) row_interval(ci, ci.box[1] + r % by, ci.box[2] + r / by, vs, r0, xa, xb);
+        uint32_t off, total;
+        Scan(scan_tmp).ExclusiveSum((uint32_t)(xb - xa), off, total);
+        s_roff[threadIdx.x] = off;
+        s_rx[threadIdx.x] = xa;
+        if (threadIdx.x == 0) s_roff[kColThreads] = total;
+        __syncthreads();
+        for (uint32_t f0 = 0; f0 < total; f0 += kColChunk) {
+            // 1. candidate test, kPerThread consecutive voxels per thread
+            uint32_t flags = 0, cnt = 0;
+            int vox[kPerThread];
 #pragma unroll
-        for (int q = 0; q < kPerThread; q++) {
-            const long long i = i0 + (long long)threadIdx.x * kPerThread + q;
-            if (i < n) {
-                const int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by),
-                          z = ci.box[2] + (int)(i / bxy);
-                if (candidate(ci, make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z), hdiag,
-                              extent)) {
-                    flags |= 1u << q;
-                    cnt++;
+            for (int q = 0; q < kPerThread; q++) {
+                const uint32_t f = f0 + threadIdx.x * kPerThread + q;
+                vox[q] = -1;
+                if (f < total) {
+                    int lo = 0, hi = kColThreads;  // last row whose start is <= f
+                    while (hi - lo > 1) {
+                        const int mid = (lo + hi) >> 1;
+                        if (s_roff[mid] <= f) lo = mid; else hi = mid;
+                    }
+                    const int rr = r0w + lo;
+                    const int x = s_rx[lo] + (int)(f - s_roff[lo]), y = ci.box[1] + rr % by, z = ci.box[2] + rr / by;
+                    if (candidate(ci, make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z), hdiag,
+                                  extent)) {
+                        flags |= 1u << q;
+                        cnt++;
+                        vox[q] = x + nx * (y + ny * z);
+                    }
                 }
             }
-        }
-        uint32_t pos, n_cand;
-        Scan(scan_tmp).ExclusiveSum(cnt, pos, n_cand);
+            uint32_t pos, n_cand;
+            Scan(scan_tmp).ExclusiveSum(cnt, pos, n_cand);
 #pragma unroll
-        for (int q = 0; q < kPerThread; q++)
-            if (flags & (1u << q)) s_cand[pos++] = (int)(threadIdx.x * kPerThread + q);
-        __syncthreads();
-        // 2. values of the candidates, spread over all threads
-        for (uint32_t k = threadIdx.x; k < n_cand; k += kColThreads) {
-            const long long i = i0 + s_cand[k];
-            const int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by), z = ci.box[2] + (int)(i / bxy);
-            s_val[k] = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
-        }
-        __syncthreads();
-        // 3. nonzeros in order into the row's segment
-        uint32_t nzc = 0;
-#pragma unroll
-        for (int q = 0; q < kPerThread; q++) {
-            const uint32_t k = threadIdx.x * kPerThread + q;
-            if (k < n_cand && s_val[k] != 0.0f) nzc++;
-        }
-        uint32_t npos, n_nz;
-        Scan(scan_tmp).ExclusiveSum(nzc, npos, n_nz);
-#pragma unroll
-        for (int q = 0; q < kPerThread; q++) {
-            const uint32_t k = threadIdx.x * kPerThread + q;
-            if (k < n_cand && s_val[k] != 0.0f) {
-                const long long i = i0 + s_cand[k];
-                const int x = ci.box[0] + (int)(i % bx), y = ci.box[1] + (int)((i / bx) % by),
-                          z = ci.box[2] + (int)(i / bxy);
-                if (written + npos < cap) {
-                    tmp_col[base + written + npos] = x + nx * (y + ny * z);
-                    tmp_val[base + written + npos] = s_val[k];
-                }
-                vmax = fmaxf(vmax, fabsf(s_val[k]));
-                npos++;
+            for (int q = 0; q < kPerThread; q++)
+                if (flags & (1u << q)) s_cand[pos++] = vox[q];
+            __syncthreads();
+            // 2. values of the candidates, spread over all threads
+            for (uint32_t k = threadIdx.x; k < n_cand; k += kColThreads) {
+                const int v = s_cand[k];
+                const int x = v % nx, y = (v / nx) % ny, z = v / (nx * ny);
+                s_val[k] = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
             }
+            __syncthreads();
+            // 3. nonzeros in order into the row's segment
+            uint32_t nzc = 0;
+#pragma unroll
+            for (int q = 0; q < kPerThread; q++) {
+                const uint32_t k = threadIdx.x * kPerThread + q;
+                if (k < n_cand && s_val[k] != 0.0f) nzc++;
+            }
+            uint32_t npos, n_nz;
+            Scan(scan_tmp).ExclusiveSum(nzc, npos, n_nz);
+#pragma unroll
+            for (int q = 0; q < kPerThread; q++) {
+                const uint32_t k = threadIdx.x * kPerThread + q;
+                if (k < n_cand && s_val[k] != 0.0f) {
+                    if (written + npos < cap) {
+                        tmp_col[base + written + npos] = s_cand[k];
+                        tmp_val[base + written + npos] = s_val[k];
+                    }
+                    vmax = fmaxf(vmax, fabsf(s_val[k]));
+                    npos++;
+                }
+            }
+            written += n_nz;
+            __syncthreads();  // s_cand / s_val / scan_tmp reuse
         }
-        written += n_nz;
-        __syncthreads();  // s_cand / s_val / scan_tmp reuse
+        __syncthreads();  // s_roff / s_rx reuse
     }
     float m = RMax(max_tmp).Reduce(vmax, cub::Max());
     if (threadIdx.x == 0) {
