@@ -5,15 +5,16 @@
 
 namespace fd2 {
 
-int ctx_scratch(fd2_context* ctx, size_t bytes, void** out) {
-    if (bytes > ctx->scratch_bytes) {
-        if (ctx->scratch) FD2_CHECK_CUDA(cudaFree(ctx->scratch));
-        ctx->scratch = nullptr;
-        ctx->scratch_bytes = 0;
-        FD2_CHECK_CUDA(cudaMalloc(&ctx->scratch, bytes));
-        ctx->scratch_bytes = bytes;
+int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, void** out) {
+    FD2_REQUIRE(slot >= 0 && slot < kBufCount, FD2_ERR_INVALID_ARGUMENT, "ctx_buffer: slot %d", slot);
+    if (bytes > ctx->buf_bytes[slot]) {
+        if (ctx->buf[slot]) FD2_CHECK_CUDA(cudaFree(ctx->buf[slot]));
+        ctx->buf[slot] = nullptr;
+        ctx->buf_bytes[slot] = 0;
+        FD2_CHECK_CUDA(cudaMalloc(&ctx->buf[slot], bytes));
+        ctx->buf_bytes[slot] = bytes;
     }
-    *out = ctx->scratch;
+    *out = ctx->buf[slot];
     return FD2_OK;
 }
 
@@ -37,12 +38,21 @@ int fd2_context_create(int device, fd2_context** out) {
         return FD2_ERR_CUDA;
     }
     c->sm_count = prop.multiProcessorCount;
+    cudaMemPoolProps pp = {};
+    pp.allocType = cudaMemAllocationTypePinned;
+    pp.handleTypes = cudaMemHandleTypeNone;
+    pp.location.type = cudaMemLocationTypeDevice;
+    pp.location.id = device;
+    const uint64_t keep = ~0ull;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaMalloc(&c->d_status, sizeof(fd2::DeviceStatus)) != cudaSuccess ||
-        cudaMemset(c->d_status, 0, sizeof(fd2::DeviceStatus)) != cudaSuccess) {
-        fd2::set_error("context_create: stream/status allocation failed");
+        cudaMemset(c->d_status, 0, sizeof(fd2::DeviceStatus)) != cudaSuccess ||
+        cudaMemPoolCreate(&c->pool, &pp) != cudaSuccess ||
+        cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess) {
+        fd2::set_error("context_create: stream/status/pool allocation failed");
         if (c->stream) cudaStreamDestroy(c->stream);
         if (c->d_status) cudaFree(c->d_status);
+        if (c->pool) cudaMemPoolDestroy(c->pool);
         delete c;
         return FD2_ERR_CUDA;
     }
@@ -53,9 +63,14 @@ int fd2_context_create(int device, fd2_context** out) {
 int fd2_context_destroy(fd2_context* c) {
     if (!c) return FD2_OK;
     cudaSetDevice(c->device);
-    if (c->scratch) cudaFree(c->scratch);
+    for (void* b : c->buf)
+        if (b) cudaFree(b);
     if (c->d_status) cudaFree(c->d_status);
     if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->pool) {
+        cudaDeviceSynchronize();  // stream-ordered frees on other streams complete first
+        cudaMemPoolDestroy(c->pool);
+    }
     delete c;
     return FD2_OK;
 }

@@ -10,6 +10,7 @@
 // Two small device->host reads per batch (row capacities, row nnz) size the
 // buffers; there is no dense beamlets x voxels matrix.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <fstream>
@@ -31,6 +32,8 @@ struct fd2_csr_ensemble {
     int32_t* d_col = nullptr;        // [cap]
     void* d_val = nullptr;           // [cap]
     float* d_scale = nullptr;        // [n_rows] (16-bit formats)
+    cudaStream_t stream = nullptr;   // the arrays are allocated, grown and freed in this stream's order
+    bool verbose = false;            // per-batch progress on stdout
     uint64_t row_cap = 0, nnz_cap = 0;
 };
 
@@ -49,27 +52,32 @@ void rot_axis_d(const double p[3], const double r[3], double t, double o[3]) {
     o[0] = a; o[1] = b; o[2] = d;
 }
 
-// Grows the ensemble's device arrays (amortised doubling).
+// Grows the ensemble's device arrays (amortised growth), from the context's
+// pool and in the order of the ensemble's stream: the old contents are copied
+// and the old arrays freed asynchronously.
 int ensemble_reserve(fd2_csr_ensemble* e, uint64_t rows, uint64_t nnz) {
+    cudaStream_t st = e->stream;
+    cudaMemPool_t pool = e->ctx->pool;
     if (rows + 1 > e->row_cap) {
         uint64_t cap = std::max<uint64_t>(rows + 1, e->row_cap * 2);
         int64_t* p;
-        FD2_CHECK_CUDA(cudaMalloc(&p, cap * sizeof(int64_t)));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&p, cap * sizeof(int64_t), pool, st));
         if (e->d_row_off) {
-            FD2_CHECK_CUDA(cudaMemcpy(p, e->d_row_off, (e->n_rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice));
-            cudaFree(e->d_row_off);
+            FD2_CHECK_CUDA(cudaMemcpyAsync(p, e->d_row_off, (e->n_rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToDevice,
+                                           st));
+            FD2_CHECK_CUDA(cudaFreeAsync(e->d_row_off, st));
         } else {
-            FD2_CHECK_CUDA(cudaMemset(p, 0, sizeof(int64_t)));
+            FD2_CHECK_CUDA(cudaMemsetAsync(p, 0, sizeof(int64_t), st));
         }
         e->d_row_off = p;
         if (e->value_type != FD2_VALUES_F32) {
-            float* s;
-            FD2_CHECK_CUDA(cudaMalloc(&s, cap * sizeof(float)));
+            float* sc;
+            FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&sc, cap * sizeof(float), pool, st));
             if (e->d_scale) {
-                FD2_CHECK_CUDA(cudaMemcpy(s, e->d_scale, e->n_rows * sizeof(float), cudaMemcpyDeviceToDevice));
-                cudaFree(e->d_scale);
+                FD2_CHECK_CUDA(cudaMemcpyAsync(sc, e->d_scale, e->n_rows * sizeof(float), cudaMemcpyDeviceToDevice, st));
+                FD2_CHECK_CUDA(cudaFreeAsync(e->d_scale, st));
             }
-            e->d_scale = s;
+            e->d_scale = sc;
         }
         e->row_cap = cap;
     }
@@ -77,13 +85,14 @@ int ensemble_reserve(fd2_csr_ensemble* e, uint64_t rows, uint64_t nnz) {
         uint64_t cap = std::max<uint64_t>(nnz, e->nnz_cap + e->nnz_cap / 2);
         int32_t* c;
         void* v;
-        FD2_CHECK_CUDA(cudaMalloc(&c, cap * sizeof(int32_t)));
-        FD2_CHECK_CUDA(cudaMalloc(&v, cap * value_bytes(e->value_type)));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&c, cap * sizeof(int32_t), pool, st));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync(&v, cap * value_bytes(e->value_type), pool, st));
         if (e->d_col) {
-            FD2_CHECK_CUDA(cudaMemcpy(c, e->d_col, e->nnz * sizeof(int32_t), cudaMemcpyDeviceToDevice));
-            FD2_CHECK_CUDA(cudaMemcpy(v, e->d_val, e->nnz * value_bytes(e->value_type), cudaMemcpyDeviceToDevice));
-            cudaFree(e->d_col);
-            cudaFree(e->d_val);
+            FD2_CHECK_CUDA(cudaMemcpyAsync(c, e->d_col, e->nnz * sizeof(int32_t), cudaMemcpyDeviceToDevice, st));
+            FD2_CHECK_CUDA(
+                cudaMemcpyAsync(v, e->d_val, e->nnz * value_bytes(e->value_type), cudaMemcpyDeviceToDevice, st));
+            FD2_CHECK_CUDA(cudaFreeAsync(e->d_col, st));
+            FD2_CHECK_CUDA(cudaFreeAsync(e->d_val, st));
         }
         e->d_col = c;
         e->d_val = v;
@@ -93,8 +102,8 @@ int ensemble_reserve(fd2_csr_ensemble* e, uint64_t rows, uint64_t nnz) {
 }
 
 template <typename T>
-int upload(const std::vector<T>& h, T** d, cudaStream_t st) {
-    FD2_CHECK_CUDA(cudaMallocAsync((void**)d, std::max<size_t>(1, h.size()) * sizeof(T), st));
+int upload(const std::vector<T>& h, T** d, cudaMemPool_t pool, cudaStream_t st) {
+    FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)d, std::max<size_t>(1, h.size()) * sizeof(T), pool, st));
     if (!h.empty()) FD2_CHECK_CUDA(cudaMemcpyAsync(*d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, st));
     return FD2_OK;
 }
@@ -154,40 +163,55 @@ void make_column_info(const fd2_beam_t& b, const fd2_volume_t* vol, ColumnInfo& 
     }
 }
 
+// Candidate voxels of each beamlet (the capacity of its row): geometry only,
+// so it runs before the beamlets' dose exists.
+static int column_counts(fd2_context* ctx, const ColumnInfo* d_infos, size_t nb, const fd2_volume_t& vol, float extent,
+                         cudaStream_t st, std::vector<uint32_t>& cnt) {
+    cnt.assign(nb, 0);
+    if (!nb) return FD2_OK;
+    uint32_t* d_cnt = nullptr;
+    FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_cnt, nb * sizeof(uint32_t), ctx->pool, st));
+    int rc = launch_column_count(d_infos, nb, d_cnt, vol, extent, st);
+    cudaError_t e = rc ? cudaSuccess : cudaMemcpyAsync(cnt.data(), d_cnt, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaFreeAsync(d_cnt, st);
+    if (!rc && e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (rc) return rc;
+    FD2_CHECK_CUDA(e);
+    ctx->launches += 1;
+    return FD2_OK;
+}
+
 // Column emission of a batch of beamlets whose BEV dose is in `aD` (device
-// array of device pointers, [L][P] each): count -> values -> gather, appended
-// as rows to the ensemble.
-static int append_columns(fd2_csr_ensemble* e, const fd2_beam_t* hb, size_t nb, const float* const* aD,
-                          const fd2_volume_t& vol, float extent, int ss, cudaStream_t st) {
-    std::vector<ColumnInfo> infos(nb);
-    for (size_t k = 0; k < nb; k++) make_column_info(hb[k], &vol, infos[k]);
-    ColumnInfo* d_infos = nullptr;
-    uint32_t *d_cnt = nullptr, *d_nnz = nullptr;
+// array of device pointers, [L][P] each) and whose candidate counts are `cnt`:
+// values into the context's column buffer at capacity offsets, then gathered
+// as rows appended to the ensemble.
+static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const uint32_t* cnt, size_t nb,
+                          const float* const* aD, const fd2_volume_t& vol, float extent, int ss, cudaStream_t st) {
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
+    fd2_context* ctx = e->ctx;
+    uint32_t* d_nnz = nullptr;
     uint64_t* d_cap_off = nullptr;
     int64_t* d_roff = nullptr;
-    int32_t* d_tcol = nullptr;
-    float *d_tval = nullptr, *d_max = nullptr, *d_iscale = nullptr;
+    float *d_max = nullptr, *d_iscale = nullptr;
     int rc = [&]() -> int {
-        FD2_TRY(upload(infos, &d_infos, st));
-        // row capacities: candidate voxels per beamlet
-        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_cnt, nb * sizeof(uint32_t), st));
-        FD2_TRY(launch_column_count(d_infos, nb, d_cnt, vol, extent, st));
-        std::vector<uint32_t> cnt(nb);
-        FD2_CHECK_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
         std::vector<uint64_t> cap(nb + 1, 0);
         for (size_t k = 0; k < nb; k++) cap[k + 1] = cap[k] + cnt[k];
-        FD2_TRY(upload(cap, &d_cap_off, st));
-        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_tcol, std::max<uint64_t>(1, cap[nb]) * sizeof(int32_t), st));
-        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_tval, std::max<uint64_t>(1, cap[nb]) * sizeof(float), st));
-        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_nnz, nb * sizeof(uint32_t), st));
-        FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_max, nb * sizeof(float), st));
+        const uint64_t ncap = std::max<uint64_t>(1, cap[nb]);
+        void* tmp = nullptr;
+        FD2_TRY(ctx_buffer(ctx, kBufColumns, ncap * (sizeof(int32_t) + sizeof(float)), &tmp));
+        int32_t* d_tcol = (int32_t*)tmp;
+        float* d_tval = (float*)(d_tcol + ncap);
+        FD2_TRY(upload(cap, &d_cap_off, ctx->pool, st));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_nnz, nb * sizeof(uint32_t), ctx->pool, st));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_max, nb * sizeof(float), ctx->pool, st));
         FD2_TRY(launch_column_values(d_infos, nb, aD, d_cap_off, d_tcol, d_tval, d_nnz, d_max, vol, extent, ss, st));
         std::vector<uint32_t> nnz(nb);
         std::vector<float> vmax(nb);
         FD2_CHECK_CUDA(cudaMemcpyAsync(nnz.data(), d_nnz, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         FD2_CHECK_CUDA(cudaMemcpyAsync(vmax.data(), d_max, nb * sizeof(float), cudaMemcpyDeviceToHost, st));
         FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+        const double t_values = ms();
         // final row offsets of this batch, appended to the ensemble
         std::vector<int64_t> roff(nb + 1);
         roff[0] = (int64_t)e->nnz;
@@ -198,7 +222,7 @@ static int append_columns(fd2_csr_ensemble* e, const fd2_beam_t* hb, size_t nb, 
         FD2_TRY(ensemble_reserve(e, e->n_rows + nb, (uint64_t)roff[nb]));
         FD2_CHECK_CUDA(cudaMemcpyAsync(e->d_row_off + e->n_rows + 1, roff.data() + 1, nb * sizeof(int64_t),
                                        cudaMemcpyHostToDevice, st));
-        FD2_TRY(upload(roff, &d_roff, st));
+        FD2_TRY(upload(roff, &d_roff, ctx->pool, st));
         if (e->value_type != FD2_VALUES_F32) {
             // per-row scale: the row maximum maps to 1 (value = scale * stored)
             std::vector<float> sc(nb), isc(nb);
@@ -208,18 +232,21 @@ static int append_columns(fd2_csr_ensemble* e, const fd2_beam_t* hb, size_t nb, 
             }
             FD2_CHECK_CUDA(
                 cudaMemcpyAsync(e->d_scale + e->n_rows, sc.data(), nb * sizeof(float), cudaMemcpyHostToDevice, st));
-            FD2_TRY(upload(isc, &d_iscale, st));
+            FD2_TRY(upload(isc, &d_iscale, ctx->pool, st));
         }
         FD2_TRY(launch_column_gather(nb, d_cap_off, d_roff, d_tcol, d_tval, d_iscale, e->d_col, e->d_val,
                                      e->value_type, st));
         FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+        if (e->verbose)
+            std::printf("  columns: %zu beamlets, candidates %llu, nnz %lld; host ms: values done %.1f, gathered "
+                        "%.1f\n",
+                        nb, (unsigned long long)cap[nb], (long long)(roff[nb] - roff[0]), t_values, ms());
         e->n_rows += nb;
         e->nnz = (uint64_t)roff[nb];
-        e->ctx->launches += 3;  // count, values, gather
+        ctx->launches += 2;  // values, gather
         return FD2_OK;
     }();
-    for (void* p : {(void*)d_infos, (void*)d_cnt, (void*)d_nnz, (void*)d_cap_off, (void*)d_roff, (void*)d_tcol,
-                    (void*)d_tval, (void*)d_max, (void*)d_iscale})
+    for (void* p : {(void*)d_nnz, (void*)d_cap_off, (void*)d_roff, (void*)d_max, (void*)d_iscale})
         if (p) cudaFreeAsync(p, st);
     return rc;
 }
@@ -300,23 +327,44 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
 
     auto* e = new fd2_csr_ensemble();
     e->ctx = ctx;
+    e->stream = st;
+    e->verbose = params.verbose != 0;
     e->n_cols = nvox;
     e->value_type = params.value_type;
     e->mat_rows.assign(1, 0);
-    int rc = ensemble_reserve(e, 0, 0);
-    if (rc) { fd2_csr_ensemble_destroy(e); return rc; }
+    // Column geometry and candidate counts of every beamlet, before any dose:
+    // their sum bounds the matrix, which is then allocated once.
+    std::vector<ColumnInfo> infos(total);
+    for (size_t k = 0; k < total; k++) make_column_info(beams[k], &vol, infos[k]);
+    ColumnInfo* d_infos = nullptr;
+    std::vector<uint32_t> cnt;
+    int rc = upload(infos, &d_infos, ctx->pool, st);
+    if (!rc) rc = column_counts(ctx, d_infos, total, vol, params.extent, st, cnt);
+    uint64_t cap_total = 0;
+    for (uint32_t c : cnt) cap_total += c;
+    if (!rc) rc = ensemble_reserve(e, total, cap_total);
+    if (rc) {
+        if (d_infos) cudaFreeAsync(d_infos, st);
+        fd2_csr_ensemble_destroy(e);
+        return rc;
+    }
 
-    // memory budget for the BEV scratch of one batch
+    // memory budget for the BEV buffers of one batch (a fixed share of the
+    // device, so the batches and buffer sizes repeat from plan to plan)
     size_t free_b = 0, tot_b = 0;
     cudaMemGetInfo(&free_b, &tot_b);
-    size_t budget = params.memory_budget ? params.memory_budget : std::min<size_t>(free_b / 4, (size_t)16 << 30);
+    size_t budget = params.memory_budget ? params.memory_budget : std::min<size_t>(tot_b / 10, (size_t)16 << 30);
 
     float* d_fluence = nullptr;
     fd2_beam_t* d_beams = nullptr;
-    rc = upload(std::vector<float>(h_fluence, h_fluence + P), &d_fluence, st);
-    if (!rc) rc = upload(beams, &d_beams, st);
+    rc = upload(std::vector<float>(h_fluence, h_fluence + P), &d_fluence, ctx->pool, st);
+    if (!rc) rc = upload(beams, &d_beams, ctx->pool, st);
 
     size_t b0 = 0, beam0 = 0;
+    const auto t_start = std::chrono::steady_clock::now();
+    auto ms_since = [&](std::chrono::steady_clock::time_point t) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t).count();
+    };
     while (!rc && beam0 < n_beams) {
         // whole beams into the batch while the scratch fits
         size_t beam1 = beam0, b1 = b0, bytes = 0;
@@ -339,10 +387,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         std::vector<size_t> off(nb + 1, 0);
         for (size_t k = 0; k < nb; k++) off[k + 1] = off[k] + (size_t)beams[b0 + k].long_dim * P;
         float* d_bev = nullptr;
-        rc = [&]() -> int {
-            FD2_CHECK_CUDA(cudaMallocAsync((void**)&d_bev, off[nb] * 3 * sizeof(float), st));
-            return FD2_OK;
-        }();
+        rc = ctx_buffer(ctx, kBufBev, off[nb] * 3 * sizeof(float), (void**)&d_bev);
         if (rc) break;
         float *dT = d_bev, *dR = d_bev + off[nb], *dD = d_bev + 2 * off[nb];
         std::vector<const float*> hF(nb, d_fluence);
@@ -351,10 +396,10 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         const float** aF = nullptr;
         float **aT = nullptr, **aR = nullptr, **aD = nullptr;
         rc = [&]() -> int {
-            FD2_TRY(upload(hF, &aF, st));
-            FD2_TRY(upload(hT, &aT, st));
-            FD2_TRY(upload(hR, &aR, st));
-            FD2_TRY(upload(hD, &aD, st));
+            FD2_TRY(upload(hF, &aF, ctx->pool, st));
+            FD2_TRY(upload(hT, &aT, ctx->pool, st));
+            FD2_TRY(upload(hR, &aR, ctx->pool, st));
+            FD2_TRY(upload(hD, &aD, ctx->pool, st));
             FD2_CHECK_CUDA(cudaMemsetAsync(dD, 0, off[nb] * sizeof(float), st));
             {
                 StageTimer t(ctx, st, FD2_STAGE_TERMA);
@@ -369,13 +414,13 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
                 t.stop();
             }
             StageTimer t(ctx, st, FD2_STAGE_COLUMNS);
-            int r = append_columns(e, beams.data() + b0, nb, (const float* const*)aD, vol, params.extent,
-                                   params.ss_factor, st);
+            int r = append_columns(e, d_infos + b0, cnt.data() + b0, nb, (const float* const*)aD, vol,
+                                   params.extent, params.ss_factor, st);
             t.stop();
             return r;
         }();
         // release batch buffers
-        for (void* p : {(void*)d_bev, (void*)aF, (void*)aT, (void*)aR, (void*)aD})
+        for (void* p : {(void*)aF, (void*)aT, (void*)aR, (void*)aD})  // d_bev is the context's
             if (p) cudaFreeAsync(p, st);
         if (rc) break;
         // per-beam row boundaries
@@ -385,13 +430,14 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
             e->mat_rows.push_back(row);
         }
         if (params.verbose)
-            std::printf("dose matrix batch: beams %zu..%zu, %zu beamlets, nnz total %llu\n", beam0, beam1 - 1, nb,
-                        (unsigned long long)e->nnz);
+            std::printf("dose matrix batch: beams %zu..%zu, %zu beamlets, nnz total %llu, host %.1f ms since start\n",
+                        beam0, beam1 - 1, nb, (unsigned long long)e->nnz, ms_since(t_start));
         b0 = b1;
         beam0 = beam1;
     }
     if (d_fluence) cudaFreeAsync(d_fluence, st);
     if (d_beams) cudaFreeAsync(d_beams, st);
+    if (d_infos) cudaFreeAsync(d_infos, st);
     cudaStreamSynchronize(st);
     if (!rc) {
         fd2::DeviceStatus ds;
@@ -426,16 +472,27 @@ int fd2_bev2pvcs_interp(fd2_context* ctx, size_t n_beams, const uint32_t* n_per_
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     auto* e = new fd2_csr_ensemble();
     e->ctx = ctx;
+    e->stream = st;
+    e->verbose = params.verbose != 0;
     e->n_cols = nvox;
     e->value_type = params.value_type;
     e->mat_rows.assign(1, 0);
     int rc = ensemble_reserve(e, 0, 0);
     size_t b0 = 0;
     for (size_t i = 0; !rc && i < n_beams; i++) {
-        if (n_per_beam[i])
-            rc = append_columns(e, h_beamlets + b0, n_per_beam[i], d_dose_bev + b0, vol, params.extent,
-                                params.ss_factor, st);
-        b0 += n_per_beam[i];
+        const size_t nb = n_per_beam[i];
+        if (nb) {
+            std::vector<ColumnInfo> infos(nb);
+            for (size_t k = 0; k < nb; k++) make_column_info(h_beamlets[b0 + k], &vol, infos[k]);
+            ColumnInfo* d_infos = nullptr;
+            std::vector<uint32_t> cnt;
+            rc = upload(infos, &d_infos, ctx->pool, st);
+            if (!rc) rc = column_counts(ctx, d_infos, nb, vol, params.extent, st, cnt);
+            if (!rc) rc = append_columns(e, d_infos, cnt.data(), nb, d_dose_bev + b0, vol, params.extent,
+                                         params.ss_factor, st);
+            if (d_infos) cudaFreeAsync(d_infos, st);
+        }
+        b0 += nb;
         e->mat_rows.push_back(e->n_rows);
     }
     if (rc) {
@@ -469,6 +526,7 @@ int fd2_csr_ensemble_device(const fd2_csr_ensemble* e, const int64_t** row_offse
 
 int fd2_csr_ensemble_to_host(const fd2_csr_ensemble* e, int64_t* row_offsets, int32_t* columns, float* values) {
     FD2_REQUIRE(e, FD2_ERR_INVALID_ARGUMENT, "ensemble_to_host: null ensemble");
+    FD2_CHECK_CUDA(cudaStreamSynchronize(e->stream));
     if (row_offsets)
         FD2_CHECK_CUDA(cudaMemcpy(row_offsets, e->d_row_off, (e->n_rows + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost));
     if (columns && e->nnz)
@@ -522,6 +580,7 @@ static int read_file(const std::string& path, std::vector<char>& out) {
 
 int fd2_csr_ensemble_tofile(const fd2_csr_ensemble* e, const char* folder) {
     FD2_REQUIRE(e && folder, FD2_ERR_INVALID_ARGUMENT, "tofile: null argument");
+    FD2_CHECK_CUDA(cudaStreamSynchronize(e->stream));
     mkdir(folder, 0755);
     const std::string dir(folder);
     const size_t nm = e->mat_rows.size() - 1;
@@ -602,10 +661,12 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
     }
     auto* e = new fd2_csr_ensemble();
     e->ctx = ctx;
+    e->stream = ctx->stream;
     e->n_cols = n_cols;
     e->value_type = value_type;
     e->mat_rows = mat_rows;
     int rc = ensemble_reserve(e, total_rows, nnz);
+    if (!rc && cudaStreamSynchronize(e->stream) != cudaSuccess) rc = FD2_ERR_CUDA;  // the arrays exist
     if (!rc) {
         cudaMemcpy(e->d_row_off, ro.data(), ro.size() * 8, cudaMemcpyHostToDevice);
         if (nnz) {
@@ -626,10 +687,8 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
 
 int fd2_csr_ensemble_destroy(fd2_csr_ensemble* e) {
     if (!e) return FD2_OK;
-    if (e->d_row_off) cudaFree(e->d_row_off);
-    if (e->d_col) cudaFree(e->d_col);
-    if (e->d_val) cudaFree(e->d_val);
-    if (e->d_scale) cudaFree(e->d_scale);
+    for (void* p : {(void*)e->d_row_off, (void*)e->d_col, e->d_val, (void*)e->d_scale})
+        if (p) cudaFreeAsync(p, e->stream);  // back to the context's pool, after the stream's pending work
     delete e;
     return FD2_OK;
 }
@@ -643,4 +702,5 @@ int fd2_beamlet_flags_save(const uint8_t* flags, size_t n, const char* path) {
 
 namespace fd2 {
 fd2_context* ensemble_context(const fd2_csr_ensemble* e) { return e->ctx; }
+cudaStream_t ensemble_stream(const fd2_csr_ensemble* e) { return e->stream; }
 }  // namespace fd2

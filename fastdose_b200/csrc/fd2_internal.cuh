@@ -60,9 +60,12 @@ struct fd2_context {
     int sm_count = 0;
     cudaStream_t stream = nullptr;          // internal work stream
     fd2::DeviceStatus* d_status = nullptr;  // device status word
-    // reusable scratch, grown on demand
-    void* scratch = nullptr;
-    size_t scratch_bytes = 0;
+    // reusable grow-only device buffers (fd2::ctx_buffer slots), kept between calls
+    void* buf[4] = {nullptr, nullptr, nullptr, nullptr};
+    size_t buf_bytes[4] = {0, 0, 0, 0};
+    // stream-ordered pool for batch buffers and dose-matrix storage; it keeps
+    // freed memory (release threshold = max) so repeated plans reuse it
+    cudaMemPool_t pool = nullptr;
     // instrumentation: kernels launched, and (when enabled) device time per stage
     uint64_t launches = 0;
     int timing = 0;
@@ -123,8 +126,13 @@ struct fd2_cccs_kernel {
 
 namespace fd2 {
 
-// Scratch helper: returns a device buffer of at least `bytes` owned by ctx.
-int ctx_scratch(fd2_context* ctx, size_t bytes, void** out);
+// Grow-only device buffers owned by a context, one per use.  A buffer is
+// reused by every later call on the context (calls on one context are
+// serialised: one host thread, work in stream order); growing it frees the old
+// one, which waits for the device.
+enum CtxBuffer { kBufCccs = 0, kBufBev = 1, kBufColumns = 2, kBufCount = 4 };
+int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, void** out);
+inline int ctx_scratch(fd2_context* ctx, size_t bytes, void** out) { return ctx_buffer(ctx, kBufCccs, bytes, out); }
 
 // Spectrum table passed by value to kernels (lives in the kernel parameter
 // space, not in process-global __constant__ memory).

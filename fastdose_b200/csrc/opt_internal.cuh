@@ -92,5 +92,7 @@ int matrix_transpose_fmt(const fd2_matrix* m, int index_format, fd2_matrix** out
 int matrix_spmv(const fd2_matrix* m, const float* d_x, float* d_y, cudaStream_t stream);
 // The context a dose-loading matrix was built on.
 fd2_context* ensemble_context(const fd2_csr_ensemble* e);
+// The stream a dose-loading matrix's arrays are ordered on.
+cudaStream_t ensemble_stream(const fd2_csr_ensemble* e);
 
 }  // namespace fd2

@@ -341,6 +341,7 @@ int fd2_voi_matrices(const fd2_csr_ensemble* dose, const int32_t* h_voxel_row, i
     FD2_TRY(fd2_csr_ensemble_device(dose, &d_off, &d_col, &d_val, &d_src_scale, nullptr));
     fd2_context* ctx = ensemble_context(dose);
     cudaStream_t st = ctx->stream;
+    FD2_CHECK_CUDA(cudaStreamSynchronize(ensemble_stream(dose)));  // the dose matrix is complete
     const int64_t rows = (int64_t)info.n_rows;
     const int src_type = info.value_type;
     if (src_type == FD2_VALUES_F32) d_src_scale = nullptr;

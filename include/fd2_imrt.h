@@ -89,7 +89,11 @@ int fd2_csr_ensemble_info(const fd2_csr_ensemble* e, fd2_csr_info_t* info);
 
 /* Device views: row_offsets int64[n_rows+1] (global), columns int32[nnz],
  * values (f32/f16/bf16)[nnz], row_scale float[n_rows] (NULL for F32),
- * mat_rows uint64[n_mats+1] (first row of each beam). */
+ * mat_rows uint64[n_mats+1] (first row of each beam).
+ * An ensemble's arrays come from the context's stream-ordered memory pool and
+ * are ordered on the stream it was built on (the construction call's stream,
+ * or the context's for fromfile): work on another stream must wait for that
+ * stream first, and the ensemble must be destroyed before that stream is. */
 int fd2_csr_ensemble_device(const fd2_csr_ensemble* e, const int64_t** row_offsets,
                             const int32_t** columns, const void** values, const float** row_scale,
                             const uint64_t** mat_rows_host);
