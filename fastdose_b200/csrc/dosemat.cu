@@ -34,6 +34,7 @@ struct fd2_csr_ensemble {
     float* d_scale = nullptr;        // [n_rows] (16-bit formats)
     cudaStream_t stream = nullptr;   // the arrays are allocated, grown and freed in this stream's order
     bool verbose = false;            // per-batch progress on stdout
+    uint64_t nnz_bound = 0;          // host-side upper bound of nnz while batches are in flight
     uint64_t row_cap = 0, nnz_cap = 0;
 };
 
@@ -181,22 +182,35 @@ static int column_counts(fd2_context* ctx, const ColumnInfo* d_infos, size_t nb,
     return FD2_OK;
 }
 
+// The exact nonzero count, read back from the last row offset.
+static int ensemble_sync_nnz(fd2_csr_ensemble* e) {
+    int64_t v = 0;
+    FD2_CHECK_CUDA(cudaMemcpyAsync(&v, e->d_row_off + e->n_rows, sizeof(int64_t), cudaMemcpyDeviceToHost, e->stream));
+    FD2_CHECK_CUDA(cudaStreamSynchronize(e->stream));
+    e->nnz = e->nnz_bound = (uint64_t)v;
+    return FD2_OK;
+}
+
 // Column emission of a batch of beamlets whose BEV dose is in `aD` (device
 // array of device pointers, [L][P] each) and whose candidate counts are `cnt`:
-// values into the context's column buffer at capacity offsets, then gathered
-// as rows appended to the ensemble.
+// values into the context's column buffer at capacity offsets, row offsets and
+// scales by a device scan, then the rows gathered into the ensemble -- all in
+// stream order, without waiting for the device (the exact nonzero count is
+// read when the matrix is complete, or when the capacity bound runs out).
 static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const uint32_t* cnt, size_t nb,
                           const float* const* aD, const fd2_volume_t& vol, float extent, int ss, cudaStream_t st) {
-    const auto t0 = std::chrono::steady_clock::now();
-    auto ms = [&]() { return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count(); };
     fd2_context* ctx = e->ctx;
     uint32_t* d_nnz = nullptr;
     uint64_t* d_cap_off = nullptr;
-    int64_t* d_roff = nullptr;
     float *d_max = nullptr, *d_iscale = nullptr;
     int rc = [&]() -> int {
         std::vector<uint64_t> cap(nb + 1, 0);
         for (size_t k = 0; k < nb; k++) cap[k + 1] = cap[k] + cnt[k];
+        if (e->nnz_bound + cap[nb] > e->nnz_cap) {  // the bound may not fit: use the exact count
+            FD2_TRY(ensemble_sync_nnz(e));
+            FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz + cap[nb]));
+        }
+        FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz_bound + cap[nb]));
         const uint64_t ncap = std::max<uint64_t>(1, cap[nb]);
         void* tmp = nullptr;
         FD2_TRY(ctx_buffer(ctx, kBufColumns, ncap * (sizeof(int32_t) + sizeof(float)), &tmp));
@@ -205,48 +219,21 @@ static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const 
         FD2_TRY(upload(cap, &d_cap_off, ctx->pool, st));
         FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_nnz, nb * sizeof(uint32_t), ctx->pool, st));
         FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_max, nb * sizeof(float), ctx->pool, st));
+        const bool half = e->value_type != FD2_VALUES_F32;
+        if (half) FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_iscale, nb * sizeof(float), ctx->pool, st));
         FD2_TRY(launch_column_values(d_infos, nb, aD, d_cap_off, d_tcol, d_tval, d_nnz, d_max, vol, extent, ss, st));
-        std::vector<uint32_t> nnz(nb);
-        std::vector<float> vmax(nb);
-        FD2_CHECK_CUDA(cudaMemcpyAsync(nnz.data(), d_nnz, nb * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-        FD2_CHECK_CUDA(cudaMemcpyAsync(vmax.data(), d_max, nb * sizeof(float), cudaMemcpyDeviceToHost, st));
-        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
-        const double t_values = ms();
-        // final row offsets of this batch, appended to the ensemble
-        std::vector<int64_t> roff(nb + 1);
-        roff[0] = (int64_t)e->nnz;
-        for (size_t k = 0; k < nb; k++) {
-            FD2_REQUIRE(nnz[k] <= cnt[k], FD2_ERR_CAPACITY, "column overflow (internal)");
-            roff[k + 1] = roff[k] + nnz[k];
-        }
-        FD2_TRY(ensemble_reserve(e, e->n_rows + nb, (uint64_t)roff[nb]));
-        FD2_CHECK_CUDA(cudaMemcpyAsync(e->d_row_off + e->n_rows + 1, roff.data() + 1, nb * sizeof(int64_t),
-                                       cudaMemcpyHostToDevice, st));
-        FD2_TRY(upload(roff, &d_roff, ctx->pool, st));
-        if (e->value_type != FD2_VALUES_F32) {
-            // per-row scale: the row maximum maps to 1 (value = scale * stored)
-            std::vector<float> sc(nb), isc(nb);
-            for (size_t k = 0; k < nb; k++) {
-                sc[k] = vmax[k] > 0 ? vmax[k] : 1.0f;
-                isc[k] = 1.0f / sc[k];
-            }
-            FD2_CHECK_CUDA(
-                cudaMemcpyAsync(e->d_scale + e->n_rows, sc.data(), nb * sizeof(float), cudaMemcpyHostToDevice, st));
-            FD2_TRY(upload(isc, &d_iscale, ctx->pool, st));
-        }
+        int64_t* d_roff = e->d_row_off + e->n_rows;  // [0] is this batch's first offset
+        FD2_TRY(launch_column_rows(nb, d_nnz, d_max, d_roff, half ? e->d_scale + e->n_rows : nullptr, d_iscale, st));
         FD2_TRY(launch_column_gather(nb, d_cap_off, d_roff, d_tcol, d_tval, d_iscale, e->d_col, e->d_val,
                                      e->value_type, st));
-        FD2_CHECK_CUDA(cudaStreamSynchronize(st));
-        if (e->verbose)
-            std::printf("  columns: %zu beamlets, candidates %llu, nnz %lld; host ms: values done %.1f, gathered "
-                        "%.1f\n",
-                        nb, (unsigned long long)cap[nb], (long long)(roff[nb] - roff[0]), t_values, ms());
         e->n_rows += nb;
-        e->nnz = (uint64_t)roff[nb];
-        ctx->launches += 2;  // values, gather
+        e->nnz_bound += cap[nb];
+        ctx->launches += 3;  // values, row offsets, gather
+        if (e->verbose)
+            std::printf("  columns: %zu beamlets, %llu candidates enqueued\n", nb, (unsigned long long)cap[nb]);
         return FD2_OK;
     }();
-    for (void* p : {(void*)d_nnz, (void*)d_cap_off, (void*)d_roff, (void*)d_max, (void*)d_iscale})
+    for (void* p : {(void*)d_nnz, (void*)d_cap_off, (void*)d_max, (void*)d_iscale})
         if (p) cudaFreeAsync(p, st);
     return rc;
 }
@@ -430,14 +417,15 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
             e->mat_rows.push_back(row);
         }
         if (params.verbose)
-            std::printf("dose matrix batch: beams %zu..%zu, %zu beamlets, nnz total %llu, host %.1f ms since start\n",
-                        beam0, beam1 - 1, nb, (unsigned long long)e->nnz, ms_since(t_start));
+            std::printf("dose matrix batch: beams %zu..%zu, %zu beamlets, nnz bound %llu, host %.1f ms since start\n",
+                        beam0, beam1 - 1, nb, (unsigned long long)e->nnz_bound, ms_since(t_start));
         b0 = b1;
         beam0 = beam1;
     }
     if (d_fluence) cudaFreeAsync(d_fluence, st);
     if (d_beams) cudaFreeAsync(d_beams, st);
     if (d_infos) cudaFreeAsync(d_infos, st);
+    if (!rc) rc = ensemble_sync_nnz(e);  // the one wait of the construction, besides the candidate counts
     cudaStreamSynchronize(st);
     if (!rc) {
         fd2::DeviceStatus ds;
@@ -495,6 +483,7 @@ int fd2_bev2pvcs_interp(fd2_context* ctx, size_t n_beams, const uint32_t* n_per_
         b0 += nb;
         e->mat_rows.push_back(e->n_rows);
     }
+    if (!rc) rc = ensemble_sync_nnz(e);
     if (rc) {
         fd2_csr_ensemble_destroy(e);
         return rc;
@@ -674,7 +663,7 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
             cudaMemcpy(e->d_val, b_val.data(), nnz * 4, cudaMemcpyHostToDevice);
         }
         e->n_rows = total_rows;
-        e->nnz = nnz;
+        e->nnz = e->nnz_bound = nnz;
         if (cudaDeviceSynchronize() != cudaSuccess) rc = FD2_ERR_CUDA;
     }
     if (rc) {

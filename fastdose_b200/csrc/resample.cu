@@ -336,7 +336,46 @@ __global__ void column_gather_kernel(const uint64_t* __restrict__ cap_off, const
     }
 }
 
+// Row offsets of a batch from its per-row nonzero counts, on the device:
+// row_off[0] holds the batch's first offset; row_off[1..n] = row_off[0] +
+// inclusive prefix sums.  For 16-bit values also the row scales (row maximum,
+// 1 for an empty row) and their reciprocals.
+__global__ void __launch_bounds__(1024) column_rows_kernel(const uint32_t* __restrict__ nnz,
+                                                           const float* __restrict__ vmax, int64_t n,
+                                                           int64_t* __restrict__ row_off, float* __restrict__ scale,
+                                                           float* __restrict__ inv_scale) {
+    typedef cub::BlockScan<int64_t, 1024> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ int64_t s_carry;
+    if (threadIdx.x == 0) s_carry = row_off[0];
+    __syncthreads();
+    for (int64_t i0 = 0; i0 < n; i0 += 1024) {
+        const int64_t i = i0 + threadIdx.x;
+        int64_t incl, total;
+        Scan(tmp).InclusiveSum(i < n ? (int64_t)nnz[i] : 0, incl, total);
+        if (i < n) {
+            row_off[i + 1] = s_carry + incl;
+            if (scale) {
+                const float sc = vmax[i] > 0.0f ? vmax[i] : 1.0f;
+                scale[i] = sc;
+                inv_scale[i] = 1.0f / sc;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) s_carry += total;
+        __syncthreads();
+    }
+}
+
 }  // namespace
+
+int launch_column_rows(size_t n, const uint32_t* d_nnz, const float* d_max, int64_t* d_row_off, float* d_scale,
+                       float* d_inv_scale, cudaStream_t stream) {
+    if (!n) return FD2_OK;
+    column_rows_kernel<<<1, 1024, 0, stream>>>(d_nnz, d_max, (int64_t)n, d_row_off, d_scale, d_inv_scale);
+    FD2_CHECK_CUDA(cudaGetLastError());
+    return FD2_OK;
+}
 
 int launch_bev2pvcs(const ColumnInfo& ci, const fd2_volume_t& v, const float* d_bev, float* d_out, size_t pitch,
                     int ss, float extent, cudaStream_t stream) {

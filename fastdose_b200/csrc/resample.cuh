@@ -30,6 +30,8 @@ int launch_column_count(const ColumnInfo* d_infos, size_t n, uint32_t* d_counts,
 int launch_column_values(const ColumnInfo* d_infos, size_t n, const float* const* d_dose, const uint64_t* d_cap_off,
                          int32_t* d_tmp_col, float* d_tmp_val, uint32_t* d_row_nnz, float* d_row_max,
                          const fd2_volume_t& v, float extent, int ss, cudaStream_t stream);
+int launch_column_rows(size_t n, const uint32_t* d_nnz, const float* d_max, int64_t* d_row_off, float* d_scale,
+                       float* d_inv_scale, cudaStream_t stream);
 int launch_column_gather(size_t n, const uint64_t* d_cap_off, const int64_t* d_row_off, const int32_t* d_tmp_col,
                          const float* d_tmp_val, const float* d_inv_scale, int32_t* d_col, void* d_val,
                          int value_type, cudaStream_t stream);
