@@ -268,6 +268,102 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
     return out
 
 
+def served_requests(ctx, n_requests, seed=11):
+    """Seeded plan requests of the served benchmark: a torso phantom whose
+    sides are drawn from 96..256 voxels (2.5 mm), 1..50 beams from the 4pi
+    sphere, 16x16 beamlet maps masked to the PTV."""
+    from fastdose_b200 import api, phantoms
+    from fastdose_b200.types import make_bundle
+
+    rng = np.random.default_rng(seed)
+    angles = phantoms.sphere_beam_angles(400)
+    reqs = []
+    for i in range(n_requests):
+        dim = tuple(int(v) for v in rng.integers(96, 257, size=3))
+        ph = phantoms.torso_phantom(seed=100 + i, dim=dim, ptv_radius=2.5, ptv_offset=(1.5, 1.0, 0.0))
+        iso = phantoms.mask_centroid(ph.masks["PTV"], ph.voxel)
+        sel = rng.choice(len(angles), size=int(rng.integers(1, 51)), replace=False)
+        bundles = np.array([make_bundle(iso, angles[j], sad=100.0, fluence_dim=16, beamlet_size=0.5,
+                                        sub_fluence_dim=16, sub_fluence_on=4, long_spacing=0.25) for j in sel])
+        flags = api.beamletFlagInit(ctx, bundles, ph.masks["PTV"], ph.volume)
+        beams = [api.bundle_beamlets(b, f, ph.volume) for b, f in zip(bundles, flags)]
+        beams = [b for b in beams if len(b)]
+        if beams:
+            reqs.append(dict(phantom=ph, beams=beams, fluence=api.beamlet_fluence(bundles[0])))
+    return reqs
+
+
+def served_leg(ctx, rates=(2.0, 10.0), n_requests=16, seed=11):
+    """p50/p99 plan latency (arrival -> dose-loading matrix on the device) and
+    beamlets/s of the service under Poisson arrivals, and of the plain form --
+    the same requests one beam per construction call, one request at a time --
+    replayed through the same arrivals as a FIFO single server with its
+    measured service times."""
+    import threading
+
+    import torch
+
+    from fastdose_b200 import api, phantoms, service
+
+    spec, kern = phantoms.synthetic_spectrum(), phantoms.synthetic_kernel()
+    reqs = served_requests(ctx, n_requests, seed)
+    n_bl = [sum(len(b) for b in r["beams"]) for r in reqs]
+    out = {"workload": f"{len(reqs)} requests: torso sides U[96,256] at 2.5 mm, 1-50 beams, 16x16 PTV-masked "
+                       f"beamlets ({sum(n_bl)} beamlets), 8x6 cones; Poisson arrivals",
+           "beamlets": int(sum(n_bl))}
+    # plain form: measured service time of each request, one beam per call
+    kk, ss = api.Kernel(ctx, kern), api.Spectrum(ctx, spec)
+    st = torch.cuda.current_stream()
+    service_s = []
+    for r in reqs:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        d = api.Density(ctx, r["phantom"].density, r["phantom"].volume)
+        for b in r["beams"]:
+            api.DoseMatConstruction(ctx, [b], r["fluence"], d, ss, kk, stream=st).close()
+        torch.cuda.synchronize()
+        service_s.append(time.perf_counter() - t0)
+    rng = np.random.default_rng(seed + 1)
+    for lam in rates:
+        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
+        # the plain form as a FIFO single server
+        end, lat = 0.0, []
+        for a, s in zip(arrivals, service_s):
+            end = max(end, a) + s
+            lat.append(end - a)
+        plain = {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
+                 "beamlets_per_s": sum(n_bl) / (end - arrivals[0])}
+        # the service
+        svc = service.Service(device=torch.cuda.current_device(), workers=2)
+        tickets = [None] * len(reqs)
+        t_base = svc.clock_ms()
+
+        def submitter():
+            for i, (a, r) in enumerate(zip(arrivals, reqs)):
+                delay = t_base + 1e3 * a - svc.clock_ms()
+                if delay > 0:
+                    time.sleep(delay * 1e-3)
+                tickets[i] = svc.submit(r["phantom"], r["beams"], r["fluence"], spec, kern)
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        stats = []
+        for t in tickets:
+            m, s = svc.wait(t)
+            m.close()
+            stats.append(s)
+        svc.close()
+        lat = np.array([s["end_ms"] - s["submit_ms"] for s in stats])
+        span_s = (max(s["end_ms"] for s in stats) - min(s["submit_ms"] for s in stats)) * 1e-3
+        out[f"rate_{lam:g}_per_s"] = {
+            "service": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                        "queue_p50_ms": float(np.percentile([s["start_ms"] - s["submit_ms"] for s in stats], 50)),
+                        "beamlets_per_s": sum(n_bl) / span_s, "workers": 2},
+            "plain_single_beam": plain}
+    return out
+
+
 def single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream, n_beams=20):
     """The plain single-beam form: the same beams one DoseMatConstruction call
     (one beam) at a time, as the reference's per-beam loop runs them."""
@@ -423,6 +519,7 @@ def run_fd2(args, rank, world):
         sb["batched_speedup"] = value / world / sb["value"]
         line["single_beam"] = sb
         line["optimizer"] = optimizer_leg(ctx, args.opt_iters, args.opt_rows)
+        line["served"] = served_leg(ctx)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, os.cpu_count() or 1)
     if rank == 0:
@@ -442,14 +539,19 @@ def main():
     ap.add_argument("--opt-iters", type=int, default=40)
     ap.add_argument("--opt-rows", type=int, default=2_500_000)
     ap.add_argument("--only-optimizer", action="store_true", help="run the optimizer leg alone (profiling)")
+    ap.add_argument("--only-served", action="store_true", help="run the served leg alone")
     args = ap.parse_args()
-    if args.only_optimizer:
+    if args.only_optimizer or args.only_served:
         import torch
 
         from fastdose_b200 import api
 
         torch.cuda.set_device(0)
-        print(json.dumps({"optimizer": optimizer_leg(api.Context(0), args.opt_iters, args.opt_rows)}), flush=True)
+        ctx = api.Context(0)
+        if args.only_optimizer:
+            print(json.dumps({"optimizer": optimizer_leg(ctx, args.opt_iters, args.opt_rows)}), flush=True)
+        else:
+            print(json.dumps({"served": served_leg(ctx)}), flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -72,6 +72,12 @@ _PROTOS = {
     "fd2_beam_weights_init": (_i, [_vp, _i64, _vp, _vp]),
     "fd2_boo_l2onehalf": (_i, [_vp, _i64, _vp, _vp, _i, _i, _i, _vp, _i, _i, _vp]),
     "fd2_polish": (_i, [_vp, _i, _i, _vp]),
+    # served dose calculation (fd2_service.h)
+    "fd2_service_create": (_i, [_vp, _vp]),
+    "fd2_service_destroy": (_i, [_vp]),
+    "fd2_service_submit": (_i, [_vp, _vp, _vp]),
+    "fd2_service_wait": (_i, [_vp, _u64, _vp, _vp]),
+    "fd2_service_clock_ms": (C.c_double, [_vp]),
 }
 
 _LIB = None

@@ -7,7 +7,7 @@ import re
 from fastdose_b200 import _lib
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-DECL = re.compile(r"^\s*(?:int|void|int64_t|uint64_t|const char\s*\*)\s+(fd2_\w+)\s*\(", re.M)
+DECL = re.compile(r"^\s*(?:int|void|double|int64_t|uint64_t|const char\s*\*)\s+(fd2_\w+)\s*\(", re.M)
 
 
 def _declared():
