@@ -36,6 +36,31 @@ def test_ctypes_prototypes_cover_the_headers():
     assert _declared() <= set(_lib._PROTOS), sorted(_declared() - set(_lib._PROTOS))
 
 
+def test_cpp_shim_compiles_links_and_runs(tmp_path):
+    """A C++ caller using the reference's names (fd2_compat.hpp) builds against
+    the library and runs its device-free calls."""
+    import shutil
+    import subprocess
+
+    if not shutil.which("g++"):
+        import pytest
+
+        pytest.skip("no g++")
+    src = tmp_path / "caller.cpp"
+    src.write_text(
+        '#include "fd2_compat.hpp"\n#include <cstdio>\n'
+        "int main() {\n"
+        "  auto f = &fastdose::DoseComputeCollective; auto g = &IMRT::DoseMatConstruction; (void)f; (void)g;\n"
+        '  std::printf("%d %s\\n", fd2_version(), fd2_status_string(FD2_ERR_ADMISSION));\n'
+        "  return 0;\n}\n")
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(_lib.LIB_PATH)
+    subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include",
+                    str(src), "-L", libdir, "-lfd2", f"-Wl,-rpath,{libdir}", "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split(maxsplit=1)
+    assert int(out[0]) == _lib.get().fd2_version() and out[1].strip()
+
+
 def test_status_strings_without_gpu():
     lib = _lib.get()
     assert lib.fd2_status_string(0)
