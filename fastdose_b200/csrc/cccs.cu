@@ -104,6 +104,15 @@ __device__ __forceinline__ bool crosses16(float b, float n) {
     return floorf(__fmul_rn(b, 0.0625f)) != floorf(__fmul_rn(n, 0.0625f));
 }
 
+// 2^x on the special-function unit (PTX ex2.approx.ftz.f32).  The attenuation
+// e^(-k p) is evaluated as 2^(-(k log2 e) p) with k log2 e formed once per
+// zenith bin: one multiply and one MUFU operation per exponential.
+__device__ __forceinline__ float exp2_sfu(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
 // the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
 // sums).  RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
@@ -162,7 +171,8 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
     }
 
     for (int t = t0; t < t1; t++) {
-        const float ka = cp.a[t], kb = cp.b[t], Aa = cp.A_a[t], Bb = cp.B_b[t];
+        const float Aa = cp.A_a[t], Bb = cp.B_b[t];
+        const float ka = -cp.a[t] * 1.4426950408889634f, kb = -cp.b[t] * 1.4426950408889634f;  // -k log2(e)
         const float4 d4 = dirs[((size_t)bi * n_tf + t) * n_phi + warp];
         const float3 d = make_float3(d4.x, d4.y, d4.z);
         float3 c = make_float3(0.5f, 0.5f, 0.0f);
@@ -218,7 +228,7 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
                         const float len = l2 * rsqrtf(l2);
                         const float2 trv = tr[mi];
                         const float p = len * trv.y;
-                        const float ea = __expf(-ka * p), eb = __expf(-kb * p);
+                        const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                         float2 acc = mydp[mi];
                         acc.x += dep;
@@ -243,7 +253,7 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
                     const float len = l2 * rsqrtf(l2);
                     const float2 trv = tr[act[j] ? mi : 0];
                     const float p = len * trv.y;
-                    const float ea = __expf(-ka * p), eb = __expf(-kb * p);
+                    const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                     const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                     if (act[j]) {
                         float2 acc = mydp[mi];
