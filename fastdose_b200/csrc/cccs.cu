@@ -113,6 +113,14 @@ __device__ __forceinline__ float exp2_sfu(float x) {
     return y;
 }
 
+// Segment length sqrt(l2) as l2 * rsqrt(l2) with the SFU reciprocal square
+// root (PTX rsqrt.approx.ftz.f32); l2 > 0 for every segment the march takes.
+__device__ __forceinline__ float seg_length(float l2) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l2));
+    return l2 * r;
+}
+
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
 // the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
 // sums).  RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
@@ -225,7 +233,7 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
                         const int mi = cx + 16 * (yc & 15);
                         const bool wrap = wrapx || (yc & 16);
                         const float l2 = dxz2 + dyp * dyp;
-                        const float len = l2 * rsqrtf(l2);
+                        const float len = seg_length(l2);
                         const float2 trv = tr[mi];
                         const float p = len * trv.y;
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
@@ -250,7 +258,7 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
                     const float dxp = (ntx - g.hx) * g.bsx * fe - (btx - g.hx) * g.bsx * fs;
                     const float dyp = (nty - g.hy) * g.bsy * fe - (bty - g.hy) * g.bsy * fs;
                     const float l2 = dxp * dxp + dyp * dyp + dzp * dzp;
-                    const float len = l2 * rsqrtf(l2);
+                    const float len = seg_length(l2);
                     const float2 trv = tr[act[j] ? mi : 0];
                     const float p = len * trv.y;
                     const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
