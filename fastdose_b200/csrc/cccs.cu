@@ -178,6 +178,11 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
         fiy[j] = (float)(r / g.fx);
     }
 
+    // register prefetch of the next slice's Terma/density (one pixel per thread)
+    const bool prefetch = g.P <= (int)blockDim.x;
+    int pf_s = -1;
+    float2 pf = make_float2(0.0f, 0.0f);
+
     for (int t = t0; t < t1; t++) {
         const float Aa = cp.A_a[t], Bb = cp.B_b[t];
         const float ka = -cp.a[t] * 1.4426950408889634f, kb = -cp.b[t] * 1.4426950408889634f;  // -k log2(e)
@@ -197,10 +202,24 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
         __syncthreads();  // the previous pass has finished; s_next is visible
         int s = *s_next;
         while (s < g.L) {
-            for (int v = threadIdx.x; v < g.P; v += blockDim.x)
-                tr[v] = make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
+            if (s == pf_s) {
+                if (threadIdx.x < g.P) tr[threadIdx.x] = pf;
+            } else {
+                for (int v = threadIdx.x; v < g.P; v += blockDim.x)
+                    tr[v] = make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
+            }
             for (int v = lane; v < g.P; v += 32) mydp[v] = make_float2(0.0f, 0.0f);
             __syncthreads();
+            // Prefetch the slice most likely to come next (s + 1, or slice 0 of
+            // the next zenith bin) into registers; its loads are in flight during
+            // the march and are used only if that slice is the one taken.
+            pf_s = -1;
+            if (prefetch) {
+                pf_s = s + 1 < g.L ? s + 1 : (t + 1 < t1 ? 0 : -1);
+                if (pf_s >= 0 && threadIdx.x < g.P)
+                    pf = make_float2(__ldg(T + (size_t)pf_s * pitch + threadIdx.x),
+                                     __ldg(R + (size_t)pf_s * pitch + threadIdx.x));
+            }
 
             int guard = 0;
             for (;;) {
@@ -299,7 +318,10 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
                 if (split)
                     split_out[(size_t)blockIdx.x * split_stride + (size_t)s * g.P + v] = val;
                 else
-                    D[(size_t)s * pitch + v] += val;
+                    // this block alone owns beam bi's dose and each (s, v) stays with
+                    // one thread, so a fire-and-forget add gives D + val in pass order
+                    // without waiting for D's old value
+                    atomicAdd(D + (size_t)s * pitch + v, val);
             }
             __syncthreads();  // dp and tr are read; s_next was read by every thread
             s = s_new;
