@@ -234,21 +234,27 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
         P = optimize.Problem(ctx, A, AT, Dm, DTm, n_ptv, n_oar, w["max_dose"], w["max_weights"], w["min_dose"],
                              w["min_weights"], w["oar_weights"], 1.0, 0.1)
         bw = 0.1 * P.beam_weights_init(groups)
-        # SpMV alone: A x over the whole matrix
-        x = torch.rand(cols, device="cuda")
-        y = torch.empty(rows, device="cuda")
+        # SpMV alone: A x and A^T y over the whole matrix
         s = torch.cuda.current_stream()
-        for _ in range(3):
-            A.spmv(x, y, stream=s)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 10
-        e0.record(s)
-        for _ in range(reps):
-            A.spmv(x, y, stream=s)
-        e1.record(s)
-        torch.cuda.synchronize()
-        spmv_ms = e0.elapsed_time(e1) / reps
-        spmv_bytes = info["device_bytes"] + cols * 4 + rows * 4  # matrix stream + x + y
+
+        def time_spmv(M, n_in, n_out, reps=10):
+            xv = torch.rand(n_in, device="cuda")
+            yv = torch.empty(n_out, device="cuda")
+            for _ in range(3):
+                M.spmv(xv, yv, stream=s)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            for _ in range(reps):
+                M.spmv(xv, yv, stream=s)
+            e1.record(s)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            nb = M.info()["device_bytes"] + n_in * 4 + n_out * 4  # matrix stream + x + y
+            return {"ms": ms, "bytes": nb, "gbs": nb / ms * 1e-6, "frac": nb / ms * 1e-6 / peak,
+                    "x_in_shared": M.info()["x_in_shared"]}
+
+        spmv_a = time_spmv(A, cols, rows)
+        spmv_at = time_spmv(AT, rows, cols)
         P.boo(groups, bw, x0, step_size=1e-3, iters=3, want=0, change_trigger=10 ** 9)  # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -257,8 +263,7 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
         out[key] = {"it_per_s": r["k"] / dt, "trials": r["trials"], "iters": r["k"], "loss": float(r["loss"][r["k"] - 1]),
                    "nnz": info["nnz"], "matrix_bytes": info["device_bytes"],
                    "exception_chunks": info["exception_chunks"],
-                   "spmv": {"ms": spmv_ms, "bytes": spmv_bytes, "gbs": spmv_bytes / spmv_ms * 1e-6,
-                            "frac": spmv_bytes / spmv_ms * 1e-6 / peak}}
+                   "spmv": spmv_a, "spmv_transpose": spmv_at}
         del P, A, AT
         torch.cuda.empty_cache()
     base = out["f32_i32"]

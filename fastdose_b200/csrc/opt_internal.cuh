@@ -61,11 +61,15 @@ struct fd2_matrix {
     float* d_scale = nullptr;      // [rows] or [cols] when scale_axis != NONE
     // stream SpMV plan
     int64_t n_chunks = 0;          // nnz_pad / kChunk
-    uint32_t* d_head = nullptr;    // [n_chunks * kChunkWords] bit k: nonzero k starts its row
+    uint32_t* d_head = nullptr;    // [n_chunks * kChunkWords] row starts: per chunk 32 bytes, one per
+                                   // lane; bit i of byte l: element 32 i + l starts its row
     int32_t* d_chunk_h = nullptr;  // [n_chunks] row starts before the chunk
+    int32_t* d_chunk_row0 = nullptr;  // [n_chunks] first row starting in the chunk if its starts are
+                                      // consecutive rows, else -1 - d_chunk_h[c]
     int32_t* d_nzrow = nullptr;    // [n_nzrows] rows with nonzeros, in order
     int64_t n_nzrows = 0;
     int n_warps = 0;               // SpMV warps (contiguous chunk ranges)
+    bool x_in_smem = false;        // SpMV instance: x staged in shared memory (cols small enough)
     int64_t* d_carry_row = nullptr;  // [n_warps] row open at each warp's range end
     float* d_carry_val = nullptr;    // [n_warps] its partial sum
     float* d_xs = nullptr;           // [cols] x times the column scale

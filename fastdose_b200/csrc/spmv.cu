@@ -40,12 +40,15 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kStreamThreads = 256;
 constexpr int kMaxStreamWarps = 148 * 64;  // one full wave of 64 warps per SM
+constexpr int kSmemThreads = 1024;          // x-in-shared-memory variant: one block per SM
+constexpr int64_t kSmemXMaxBytes = 200 * 1024;
 
 struct StreamArgs {
     const void* val;
     ColView cols;
     const uint32_t* head;
     const int32_t* chunk_h;
+    const int32_t* chunk_row0;
     const int32_t* nzrow;
     const float* row_scale;
     int64_t n_chunks;
@@ -53,31 +56,55 @@ struct StreamArgs {
     int64_t rows;
     int64_t* carry_row;
     float* carry_val;
+    int x_len;  // kSmemX: floats of x staged in shared memory
 };
 
-// 8 consecutive values of a lane (16-byte aligned: k is a multiple of 8)
-__device__ __forceinline__ void load8(const float* v, int64_t k, float (&o)[8]) {
-    const float4* p = reinterpret_cast<const float4*>(v + k);
-    const float4 a = __ldcs(p), b = __ldcs(p + 1);
-    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-    o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
-}
-__device__ __forceinline__ void load8(const __half* v, int64_t k, float (&o)[8]) {
-    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(v + k));
-    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
-#pragma unroll
-    for (int i = 0; i < 4; i++) {
-        const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
-        o[2 * i] = f.x;
-        o[2 * i + 1] = f.y;
+// A lane's share of one chunk as loaded, values and columns still packed, so
+// that two chunks can be in flight per warp without holding 2 x 16 unpacked
+// registers.
+template <typename T, bool kPacked>
+struct RawChunk {
+    uint4 v[sizeof(T) == 4 ? 2 : 1];  // 8 values
+    uint4 c[kPacked ? 1 : 2];         // 8 int32 columns, or 8 16-bit offsets from base
+    int base;                         // kPacked: the chunk's column base; < 0: exception chunk
+    int row0;                         // first row starting in the chunk, or -1 - (row starts before it)
+    uint32_t h;                       // this lane's row-start bits (bit i: slice i)
+};
+
+template <typename T, bool kPacked>
+__device__ __forceinline__ void load_raw(const StreamArgs& a, int64_t c, int lane, RawChunk<T, kPacked>& r) {
+    const int64_t k = c * kChunk + 8 * lane;  // 16-byte aligned: k is a multiple of 8
+    const uint4* vp = reinterpret_cast<const uint4*>(static_cast<const T*>(a.val) + k);
+    r.v[0] = __ldcs(vp);
+    if constexpr (sizeof(T) == 4) r.v[1] = __ldcs(vp + 1);
+    if constexpr (kPacked) {
+        r.base = __ldg(a.cols.cbase + c);  // one address for the warp
+        r.c[0] = __ldcs(reinterpret_cast<const uint4*>(a.cols.col16 + k));
+    } else {
+        const uint4* cp = reinterpret_cast<const uint4*>(a.cols.col + k);
+        r.c[0] = __ldcs(cp);
+        r.c[1] = __ldcs(cp + 1);
+        r.base = 0;
     }
+    r.row0 = __ldg(a.chunk_row0 + c);
+    r.h = __ldg(reinterpret_cast<const uint8_t*>(a.head) + c * (kChunk / 8) + lane);
 }
-__device__ __forceinline__ void load8(const __nv_bfloat16* v, int64_t k, float (&o)[8]) {
-    const uint4 u = __ldcs(reinterpret_cast<const uint4*>(v + k));
-    const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+
+__device__ __forceinline__ void unpack_vals(const uint4 (&u)[2], float (&o)[8]) {
+    const uint32_t w[8] = {u[0].x, u[0].y, u[0].z, u[0].w, u[1].x, u[1].y, u[1].z, u[1].w};
+#pragma unroll
+    for (int i = 0; i < 8; i++) o[i] = __uint_as_float(w[i]);
+}
+template <typename H>
+__device__ __forceinline__ void unpack_vals(const uint4 (&u)[1], float (&o)[8]) {
+    const uint32_t w[4] = {u[0].x, u[0].y, u[0].z, u[0].w};
 #pragma unroll
     for (int i = 0; i < 4; i++) {
-        const float2 f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[i]));
+        float2 f;
+        if constexpr (std::is_same<H, __half>::value)
+            f = __half22float2(*reinterpret_cast<const __half2*>(&w[i]));
+        else
+            f = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[i]));
         o[2 * i] = f.x;
         o[2 * i + 1] = f.y;
     }
@@ -90,24 +117,22 @@ __device__ __forceinline__ void load_i32x8(const int32_t* c, int64_t k, int (&o)
     o[4] = b.x; o[5] = b.y; o[6] = b.z; o[7] = b.w;
 }
 
-template <bool kPacked>
-__device__ __forceinline__ void load_cols8(const ColView& cv, int64_t chunk, int lane, int (&o)[8]) {
-    const int64_t k = chunk * kChunk + 8 * lane;
+template <typename T, bool kPacked>
+__device__ __forceinline__ void unpack_cols(const RawChunk<T, kPacked>& r, const ColView& cv, int64_t chunk, int lane,
+                                            int (&o)[8]) {
     if constexpr (!kPacked) {
-        load_i32x8(cv.col, k, o);
-    } else {
-        const int32_t base = __ldg(cv.cbase + chunk);  // one address for the warp
-        if (base >= 0) {
-            const uint4 u = __ldcs(reinterpret_cast<const uint4*>(cv.col16 + k));
-            const uint32_t w[4] = {u.x, u.y, u.z, u.w};
+        const uint32_t w[8] = {r.c[0].x, r.c[0].y, r.c[0].z, r.c[0].w, r.c[1].x, r.c[1].y, r.c[1].z, r.c[1].w};
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                o[2 * i] = base + (int)(w[i] & 0xffffu);
-                o[2 * i + 1] = base + (int)(w[i] >> 16);
-            }
-        } else {
-            load_i32x8(cv.exc, (int64_t)(-1 - base) * kChunk + 8 * lane, o);
+        for (int i = 0; i < 8; i++) o[i] = (int)w[i];
+    } else if (r.base >= 0) {
+        const uint32_t w[4] = {r.c[0].x, r.c[0].y, r.c[0].z, r.c[0].w};
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            o[2 * i] = r.base + (int)(w[i] & 0xffffu);
+            o[2 * i + 1] = r.base + (int)(w[i] >> 16);
         }
+    } else {  // a chunk whose columns span 65536 or more: int32 columns in the side array
+        load_i32x8(cv.exc, (int64_t)(-1 - r.base) * kChunk + 8 * lane, o);
     }
 }
 
@@ -120,19 +145,29 @@ __device__ __forceinline__ float warp_sum(float v) {
 }
 
 // One warp per contiguous range of chunks.  In a chunk, slice i holds logical
-// elements 32 i .. 32 i + 31 (one per lane); word i of the row-start bitmap
-// flags the lanes that start a row.  A slice without row starts only adds to
-// the open row (one FMA per lane); a slice with row starts closes the open row
-// (warp sum), sums the rows that start and end inside it with a segmented
-// warp scan, and leaves its last row open.
-template <typename T, bool kPacked>
-__global__ void __launch_bounds__(kStreamThreads) spmv_stream_kernel(StreamArgs a, const float* __restrict__ x,
-                                                                     float* __restrict__ y) {
+// elements 32 i .. 32 i + 31 (one per lane); bit i of lane l's row-start byte
+// flags element 32 i + l.  A slice without row starts only adds to the open
+// row (one FMA per lane); a slice with row starts closes the open row (warp
+// sum), sums the rows that start and end inside it with a segmented warp scan,
+// and leaves its last row open.
+//
+// kSmemX: x is copied to shared memory first (one block of kSmemThreads per
+// SM) and the gathers read it there: 32 lanes reading 32 scattered columns
+// cost a few bank cycles instead of up to 32 L1 tag lookups.  With 16-bit
+// values a warp loads ahead: the next chunk while it sums the current one (x
+// in shared memory), or two chunks at a time (x in global memory).
+template <typename T, bool kPacked, bool kSmemX>
+__global__ void __launch_bounds__(kSmemX ? kSmemThreads : kStreamThreads, kSmemX ? 1 : 4)
+    spmv_stream_kernel(StreamArgs a, const float* __restrict__ x, float* __restrict__ y) {
+    extern __shared__ float xs[];
+    if constexpr (kSmemX) {
+        for (int i = threadIdx.x; i < a.x_len; i += blockDim.x) xs[i] = __ldg(x + i);
+        __syncthreads();
+    }
     const int lane = threadIdx.x & 31;
     const int w = (int)((blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5);
     if (w >= a.n_warps) return;  // uniform per warp
     const int64_t c0 = (int64_t)w * a.n_chunks / a.n_warps, c1 = (int64_t)(w + 1) * a.n_chunks / a.n_warps;
-    const T* __restrict__ val = static_cast<const T*>(a.val);
     float oacc = 0.0f;        // this lane's share of the open row (the row in progress), this warp's part
     bool open_valid = false;  // the warp has met an element of the open row
     int open_row = 0;
@@ -140,26 +175,35 @@ __global__ void __launch_bounds__(kStreamThreads) spmv_stream_kernel(StreamArgs 
         const int hb0 = __ldg(a.chunk_h + c0);
         if (hb0 > 0 && !(__ldg(a.head + c0 * kChunkWords) & 1u)) open_row = __ldg(a.nzrow + hb0 - 1);
     }
-    for (int64_t c = c0; c < c1; c++) {
+    auto xv = [&](int col) -> float {
+        if constexpr (kSmemX)
+            return xs[col];
+        else
+            return __ldg(x + col);
+    };
+    // row of the chunk's j-th row start: consecutive rows need no lookup
+    auto row_at = [&](const RawChunk<T, kPacked>& r, int j) -> int {
+        return r.row0 >= 0 ? r.row0 + j : __ldg(a.nzrow + (-1 - r.row0) + j);
+    };
+    auto body = [&](const RawChunk<T, kPacked>& r, int64_t c) {
         float v[8];
         int col[8];
-        load8(val, c * kChunk + 8 * lane, v);
-        load_cols8<kPacked>(a.cols, c, lane, col);
-        const uint4 h0 = __ldg(reinterpret_cast<const uint4*>(a.head + c * kChunkWords));
-        const uint4 h1 = __ldg(reinterpret_cast<const uint4*>(a.head + c * kChunkWords) + 1);
-        const uint32_t hw[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
-        if (!(h0.x | h0.y | h0.z | h0.w | h1.x | h1.y | h1.z | h1.w)) {  // no row starts: all of it is the open row
+        if constexpr (sizeof(T) == 4)
+            unpack_vals(r.v, v);
+        else
+            unpack_vals<T>(r.v, v);
+        unpack_cols<T, kPacked>(r, a.cols, c, lane, col);
+        if (!__any_sync(kFull, r.h != 0u)) {  // no row starts: all of it is the open row
 #pragma unroll
-            for (int i = 0; i < 8; i++) oacc = fmaf(v[i], __ldg(x + col[i]), oacc);
+            for (int i = 0; i < 8; i++) oacc = fmaf(v[i], xv(col[i]), oacc);
             open_valid = true;
-            continue;
+            return;
         }
-        const int hbase = __ldg(a.chunk_h + c);
         int hcnt = 0;
 #pragma unroll
         for (int i = 0; i < 8; i++) {
-            const float p = v[i] * __ldg(x + col[i]);
-            const uint32_t m = hw[i];
+            const float p = v[i] * xv(col[i]);
+            const uint32_t m = __ballot_sync(kFull, (r.h >> i) & 1u);
             if (m == 0) {
                 oacc += p;
                 open_valid = true;
@@ -169,6 +213,13 @@ __global__ void __launch_bounds__(kStreamThreads) spmv_stream_kernel(StreamArgs 
             const int fh = __ffs(m) - 1;
             const float closing = warp_sum(oacc + (lane < fh ? p : 0.0f));
             if ((open_valid || fh > 0) && lane == 0) put(y, a.row_scale, open_row, closing);
+            if ((m & (m - 1u)) == 0u) {  // one row start: no row begins and ends in the slice
+                oacc = lane >= fh ? p : 0.0f;
+                hcnt += 1;
+                open_row = row_at(r, hcnt - 1);
+                open_valid = true;
+                continue;
+            }
             // rows inside the slice: segmented inclusive scan from the first start
             float s = lane >= fh ? p : 0.0f;
             int f = (m >> lane) & 1u;
@@ -182,13 +233,44 @@ __global__ void __launch_bounds__(kStreamThreads) spmv_stream_kernel(StreamArgs 
                 }
             }
             if (lane < 31 && lane >= fh && ((m >> (lane + 1)) & 1u))
-                put(y, a.row_scale, __ldg(a.nzrow + hbase + hcnt + __popc(m & ((2u << lane) - 1u)) - 1), s);
+                put(y, a.row_scale, row_at(r, hcnt + __popc(m & ((2u << lane) - 1u)) - 1), s);
             // the slice's last row stays open
             const int lh = 31 - __clz(m);
             oacc = lane >= lh ? p : 0.0f;
             hcnt += __popc(m);
-            open_row = __ldg(a.nzrow + hbase + hcnt - 1);
+            open_row = row_at(r, hcnt - 1);
             open_valid = true;
+        }
+    };
+    if constexpr (sizeof(T) == 2 && kSmemX) {
+        // 16-bit values, x in shared memory: the next chunk's loads are issued
+        // before this chunk is summed, so a warp keeps a chunk in flight while
+        // it computes
+        RawChunk<T, kPacked> r;
+        if (c0 < c1) load_raw(a, c0, lane, r);
+        for (int64_t c = c0; c < c1; c++) {
+            RawChunk<T, kPacked> rn;
+            const bool more = c + 1 < c1;  // uniform per warp
+            if (more) load_raw(a, c + 1, lane, rn);
+            body(r, c);
+            if (more) r = rn;
+        }
+    } else if constexpr (sizeof(T) == 2) {
+        // 16-bit values, x gathered from global memory: two chunks' loads are
+        // issued together (fewer registers held than the rolling form)
+        for (int64_t c = c0; c < c1; c += 2) {
+            RawChunk<T, kPacked> r0, r1;
+            load_raw(a, c, lane, r0);
+            const bool two = c + 1 < c1;  // uniform per warp
+            if (two) load_raw(a, c + 1, lane, r1);
+            body(r0, c);
+            if (two) body(r1, c + 1);
+        }
+    } else {
+        for (int64_t c = c0; c < c1; c++) {
+            RawChunk<T, kPacked> r;
+            load_raw(a, c, lane, r);
+            body(r, c);
         }
     }
     const float part = warp_sum(oacc);
@@ -223,14 +305,36 @@ unsigned grid_for(int64_t n, int threads = 256) {
     return (unsigned)std::max<int64_t>(1, std::min<int64_t>((n + threads - 1) / threads, 148 * 16));
 }
 
-// bit off[r] of the row-start bitmap for every row with nonzeros (rows own
-// distinct bits; atomicOr makes the word updates safe)
+// the row-start bit of off[r] for every row with nonzeros (rows own distinct
+// bits; atomicOr makes the word updates safe).  Layout: a chunk has 32 bytes,
+// one per lane; bit i of byte l flags logical element 32 i + l.
 __global__ void mark_row_starts(const int64_t* __restrict__ off, int64_t rows, uint32_t* __restrict__ head,
                                 int32_t* __restrict__ nonempty) {
     for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < rows; r += (int64_t)gridDim.x * blockDim.x) {
         const bool ne = off[r + 1] > off[r];
         nonempty[r] = ne;
-        if (ne) atomicOr(head + off[r] / 32, 1u << (off[r] % 32));
+        if (ne) {  // element e of chunk c: lane e % 32's byte, bit e / 32
+            const int64_t c = off[r] / kChunk;
+            const int e = (int)(off[r] % kChunk), l = e & 31;
+            atomicOr(head + c * kChunkWords + (l >> 2), 1u << ((l & 3) * 8 + (e >> 5)));
+        }
+    }
+}
+
+// Per chunk: the row of its first row start when all its row starts belong to
+// consecutive rows (no empty row between them), so the j-th is row0 + j;
+// otherwise -1 - (row starts before the chunk), and the rows come from nzrow.
+__global__ void chunk_first_rows(const int32_t* __restrict__ cnt, const int32_t* __restrict__ chunk_h,
+                                 const int32_t* __restrict__ nzrow, int64_t n_chunks, int32_t* __restrict__ row0) {
+    for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < n_chunks;
+         c += (int64_t)gridDim.x * blockDim.x) {
+        const int n = cnt[c], hb = chunk_h[c];
+        if (n == 0) {
+            row0[c] = 0;  // no row starts: never read
+            continue;
+        }
+        const int r0 = nzrow[hb];
+        row0[c] = nzrow[hb + n - 1] - r0 == n - 1 ? r0 : -1 - hb;
     }
 }
 
@@ -413,17 +517,36 @@ __global__ void gather_transposed(const int64_t* __restrict__ off, int64_t rows,
     }
 }
 
+// The x-in-shared-memory instance of the stream kernel, allowed the largest x.
+template <typename T, bool kPacked>
+cudaError_t allow_smem_x() {
+    return cudaFuncSetAttribute(spmv_stream_kernel<T, kPacked, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSmemXMaxBytes);
+}
+
+template <typename T, bool kPacked>
+int launch_stream_fmt(const fd2_matrix* m, const StreamArgs& a, const float* x, float* y, cudaStream_t st) {
+    if (m->x_in_smem) {
+        FD2_CHECK_CUDA((allow_smem_x<T, kPacked>()));
+        const unsigned blocks = (unsigned)(((int64_t)m->n_warps * 32 + kSmemThreads - 1) / kSmemThreads);
+        spmv_stream_kernel<T, kPacked, true><<<blocks, kSmemThreads, (size_t)m->cols * sizeof(float), st>>>(a, x, y);
+    } else {
+        const unsigned blocks = (unsigned)(((int64_t)m->n_warps * 32 + kStreamThreads - 1) / kStreamThreads);
+        spmv_stream_kernel<T, kPacked, false><<<blocks, kStreamThreads, 0, st>>>(a, x, y);
+    }
+    FD2_CHECK_CUDA(cudaGetLastError());
+    return FD2_OK;
+}
+
 template <typename T>
 int launch_stream(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) {
-    StreamArgs a{m->d_val, m->cols_view(), m->d_head, m->d_chunk_h, m->d_nzrow,
+    StreamArgs a{m->d_val, m->cols_view(), m->d_head, m->d_chunk_h, m->d_chunk_row0, m->d_nzrow,
                  m->scale_axis == FD2_SCALE_ROWS ? m->d_scale : nullptr, m->n_chunks, m->n_warps, m->rows,
-                 m->d_carry_row, m->d_carry_val};
-    const unsigned blocks = (unsigned)(((int64_t)m->n_warps * 32 + kStreamThreads - 1) / kStreamThreads);
+                 m->d_carry_row, m->d_carry_val, (int)m->cols};
     if (m->index_format == FD2_INDEX_PACKED16)
-        spmv_stream_kernel<T, true><<<blocks, kStreamThreads, 0, st>>>(a, x, y);
+        FD2_TRY((launch_stream_fmt<T, true>(m, a, x, y, st)));
     else
-        spmv_stream_kernel<T, false><<<blocks, kStreamThreads, 0, st>>>(a, x, y);
-    FD2_CHECK_CUDA(cudaGetLastError());
+        FD2_TRY((launch_stream_fmt<T, false>(m, a, x, y, st)));
     spmv_fixup_kernel<<<(m->n_warps + 255) / 256, 256, 0, st>>>(m->n_warps, m->d_carry_row, m->d_carry_val,
                                                                a.row_scale, m->rows, y);
     FD2_CHECK_CUDA(cudaGetLastError());
@@ -498,7 +621,7 @@ int matrix_alloc_entries(fd2_matrix* m, cudaStream_t st) {
 
 void matrix_free(fd2_matrix* m) {
     for (void* p : {(void*)m->d_off, (void*)m->d_col, (void*)m->d_col16, (void*)m->d_cbase, (void*)m->d_exc, m->d_val,
-                    (void*)m->d_scale, (void*)m->d_head, (void*)m->d_chunk_h, (void*)m->d_nzrow,
+                    (void*)m->d_scale, (void*)m->d_head, (void*)m->d_chunk_h, (void*)m->d_chunk_row0, (void*)m->d_nzrow,
                     (void*)m->d_carry_row, (void*)m->d_carry_val, (void*)m->d_xs})
         if (p) cudaFree(p);
     m->d_off = nullptr;
@@ -508,33 +631,47 @@ void matrix_free(fd2_matrix* m) {
     m->d_val = nullptr;
     m->d_scale = nullptr;
     m->d_head = nullptr;
-    m->d_chunk_h = m->d_nzrow = nullptr;
+    m->d_chunk_h = m->d_chunk_row0 = m->d_nzrow = nullptr;
     m->d_carry_row = nullptr;
     m->d_carry_val = m->d_xs = nullptr;
 }
 
 // Warps of one full wave of the stream kernel for this matrix's instance: every
-// warp owns one contiguous range, so there is no second, partial wave.
+// warp owns one contiguous range, so there is no second, partial wave.  A
+// matrix whose x fits in shared memory (cols x 4 bytes <= kSmemXMaxBytes) uses
+// the x-in-shared-memory instance, one block of kSmemThreads per SM.
 template <typename T, bool kPacked>
-int resident_warps(int sm_count) {
+int resident_warps(fd2_matrix* m, int sm_count) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_stream_kernel<T, kPacked>, kStreamThreads, 0) !=
-            cudaSuccess ||
+    const int64_t xb = m->cols * (int64_t)sizeof(float);
+    m->x_in_smem = false;
+    if (xb > 0 && xb <= kSmemXMaxBytes && allow_smem_x<T, kPacked>() == cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_stream_kernel<T, kPacked, true>, kSmemThreads,
+                                                      (size_t)xb) == cudaSuccess &&
+        per_sm >= 1) {
+        m->x_in_smem = true;
+        return per_sm * sm_count * (kSmemThreads / 32);
+    }
+    cudaGetLastError();  // a refused attribute or query leaves the global-gather instance
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, spmv_stream_kernel<T, kPacked, false>, kStreamThreads,
+                                                      0) != cudaSuccess ||
         per_sm < 1)
         per_sm = 1;
     return per_sm * sm_count * (kStreamThreads / 32);
 }
 
-int stream_warps(const fd2_matrix* m) {
+int stream_warps(fd2_matrix* m) {
     const int sms = m->ctx->sm_count > 0 ? m->ctx->sm_count : 148;
     const bool pk = m->index_format == FD2_INDEX_PACKED16;
     int w;
     switch (m->value_type) {
-        case FD2_VALUES_F16: w = pk ? resident_warps<__half, true>(sms) : resident_warps<__half, false>(sms); break;
-        case FD2_VALUES_BF16:
-            w = pk ? resident_warps<__nv_bfloat16, true>(sms) : resident_warps<__nv_bfloat16, false>(sms);
+        case FD2_VALUES_F16:
+            w = pk ? resident_warps<__half, true>(m, sms) : resident_warps<__half, false>(m, sms);
             break;
-        default: w = pk ? resident_warps<float, true>(sms) : resident_warps<float, false>(sms);
+        case FD2_VALUES_BF16:
+            w = pk ? resident_warps<__nv_bfloat16, true>(m, sms) : resident_warps<__nv_bfloat16, false>(m, sms);
+            break;
+        default: w = pk ? resident_warps<float, true>(m, sms) : resident_warps<float, false>(m, sms);
     }
     return std::min(w, kMaxStreamWarps);
 }
@@ -544,6 +681,7 @@ int matrix_finalize(fd2_matrix* m, cudaStream_t st) {
     m->n_warps = (int)std::max<int64_t>(1, std::min<int64_t>(m->n_chunks, stream_warps(m)));
     FD2_CHECK_CUDA(cudaMalloc(&m->d_head, std::max<int64_t>(m->n_chunks * kChunkWords, 1) * sizeof(uint32_t)));
     FD2_CHECK_CUDA(cudaMalloc(&m->d_chunk_h, std::max<int64_t>(m->n_chunks, 1) * sizeof(int32_t)));
+    FD2_CHECK_CUDA(cudaMalloc(&m->d_chunk_row0, std::max<int64_t>(m->n_chunks, 1) * sizeof(int32_t)));
     FD2_CHECK_CUDA(cudaMalloc(&m->d_carry_row, m->n_warps * sizeof(int64_t)));
     FD2_CHECK_CUDA(cudaMalloc(&m->d_carry_val, m->n_warps * sizeof(float)));
     if (m->scale_axis == FD2_SCALE_COLS)
@@ -580,6 +718,9 @@ int matrix_finalize(fd2_matrix* m, cudaStream_t st) {
     if (!rc && m->n_chunks) {
         chunk_head_counts<<<grid_for(m->n_chunks), 256, 0, st>>>(m->d_head, m->n_chunks, cnt);
         rc = exclusive_scan(cnt, m->d_chunk_h, m->n_chunks, st);
+        if (!rc)
+            chunk_first_rows<<<grid_for(m->n_chunks), 256, 0, st>>>(cnt, m->d_chunk_h, m->d_nzrow, m->n_chunks,
+                                                                   m->d_chunk_row0);
     }
     // 16-bit column packing
     if (!rc && m->index_format == FD2_INDEX_PACKED16 && m->n_chunks) {
@@ -778,13 +919,13 @@ int fd2_matrix_info(const fd2_matrix* m, fd2_matrix_info_t* info) {
     info->value_type = m->value_type;
     info->scale_axis = m->scale_axis;
     info->index_format = m->index_format;
-    info->reserved = 0;
+    info->x_in_shared = m->x_in_smem ? 1 : 0;
     info->exception_chunks = m->n_exc;
     const int64_t pad = m->n_chunks * kChunk;
     const int64_t ns = m->scale_axis == FD2_SCALE_ROWS ? m->rows : m->scale_axis == FD2_SCALE_COLS ? m->cols : 0;
     const int64_t col_bytes =
         m->index_format == FD2_INDEX_PACKED16 ? pad * 2 + m->n_chunks * 4 + m->n_exc * kChunk * 4 : pad * 4;
-    info->device_bytes = pad * (int64_t)value_size(m->value_type) + col_bytes + pad / 8 + m->n_chunks * 4 +
+    info->device_bytes = pad * (int64_t)value_size(m->value_type) + col_bytes + pad / 8 + m->n_chunks * 8 +
                          m->n_nzrows * 4 + ns * (int64_t)sizeof(float);
     return FD2_OK;
 }

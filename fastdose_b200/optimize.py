@@ -23,7 +23,7 @@ INDEX_FORMATS = {"i32": 0, "packed16": 1}
 class _MatInfo(C.Structure):
     _fields_ = [("rows", C.c_int64), ("cols", C.c_int64), ("nnz", C.c_int64), ("value_type", C.c_int32),
                 ("scale_axis", C.c_int32), ("device_bytes", C.c_int64), ("index_format", C.c_int32),
-                ("reserved", C.c_int32), ("exception_chunks", C.c_int64)]
+                ("x_in_shared", C.c_int32), ("exception_chunks", C.c_int64)]
 
 
 class _State(C.Structure):
@@ -93,7 +93,7 @@ class Matrix:
         fmt = {v: k for k, v in INDEX_FORMATS.items()}[i.index_format]
         return dict(rows=i.rows, cols=i.cols, nnz=i.nnz, value_type=i.value_type,
                     scale_axis=SCALE_AXES[i.scale_axis], device_bytes=i.device_bytes, index_format=fmt,
-                    exception_chunks=i.exception_chunks)
+                    exception_chunks=i.exception_chunks, x_in_shared=bool(i.x_in_shared))
 
     @property
     def shape(self):

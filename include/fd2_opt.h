@@ -69,7 +69,7 @@ typedef struct fd2_matrix_info {
     int32_t scale_axis;   /* fd2_scale_axis */
     int64_t device_bytes; /* bytes one SpMV pass streams: offsets/plan, columns, values, scales */
     int32_t index_format; /* fd2_index_format */
-    int32_t reserved;
+    int32_t x_in_shared; /* SpMV instance: 1 = x staged in shared memory (cols x 4 bytes <= 200 KiB) */
     int64_t exception_chunks; /* PACKED16 chunks stored with int32 columns */
 } fd2_matrix_info_t;
 

@@ -41,16 +41,22 @@ def _dense(m, rows):
     return d
 
 
+@pytest.mark.parametrize("cols,density", [(6000, 0.01), (60000, 0.001)])
 @pytest.mark.parametrize("fmt", ["i32", "packed16"])
 @pytest.mark.parametrize("vt", ["f32", "f16", "bf16"])
-def test_spmv_matches_exact_product(ctx, vt, fmt):
+def test_spmv_matches_exact_product(ctx, vt, fmt, cols, density):
+    """Both SpMV instances: x of 6000 floats is gathered from shared memory,
+    x of 60000 floats (over 200 KiB) from global memory."""
+    import scipy.sparse as sp
     import torch
 
     rng = np.random.default_rng(3)
-    rows, cols = 700, 6000  # rows 3 and 400 span many 256-nonzero chunks and several warps
-    m = _random_csr(rng, rows, cols, 0.01, long_rows=(3, 400))
+    rows = 700  # rows 3 and 400 span many 256-nonzero chunks and several warps
+    m = _random_csr(rng, rows, cols, density, long_rows=(3, 400))
     M = optimize.Matrix.from_csr(ctx, *m[:3], cols, value_type=vt, index_format=fmt)
-    assert M.info()["index_format"] == fmt
+    info = M.info()
+    assert info["index_format"] == fmt
+    assert info["x_in_shared"] == (cols * 4 <= 200 * 1024)
     off, col, val = M.to_host()  # the stored (rounded) values, scale applied
     np.testing.assert_array_equal(off, m[0])
     np.testing.assert_array_equal(col, m[1])
@@ -58,9 +64,9 @@ def test_spmv_matches_exact_product(ctx, vt, fmt):
     assert np.all(np.abs(val - m[2]) <= rel * np.abs(m[2]) + 1e-12)
     x = rng.standard_normal(cols).astype(np.float32)
     y = M.spmv(torch.from_numpy(x).cuda()).cpu().numpy()
-    D = _dense((off, col, val, cols), rows)
+    D = sp.csr_matrix((val.astype(np.float64), col, off), shape=(rows, cols))
     ref = D @ x.astype(np.float64)
-    bound = np.abs(D) @ np.abs(x.astype(np.float64))
+    bound = abs(D) @ np.abs(x.astype(np.float64))
     assert np.all(np.abs(y - ref) <= 2e-5 * bound + 1e-30)
     # empty rows are written as zero and repeated products are bit-identical
     empty = np.diff(off) == 0
