@@ -266,6 +266,7 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
                    "spmv": spmv_a, "spmv_transpose": spmv_at}
         del P, A, AT
         torch.cuda.empty_cache()
+    out["reference_form"] = reference_form_spmv(ctx, rows // 10, cols, seed, peak)
     base = out["f32_i32"]
     for key in ("f32_packed16", "f16_packed16", "bf16_packed16"):
         out[key]["speedup_vs_f32_i32"] = out[key]["it_per_s"] / base["it_per_s"]
@@ -273,6 +274,58 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
     for key in ("f16_packed16", "bf16_packed16"):
         out[key]["speedup_vs_f32_packed16"] = out[key]["it_per_s"] / out["f32_packed16"]["it_per_s"]
     return out
+
+
+def reference_form_spmv(ctx, rows, cols, seed, peak):
+    """A x in the reference's form -- cuSPARSE SpMV on FP32 values with int64
+    row offsets and column indices (MatCSR64 through cusparseSpMV, as
+    Eigen2Cusparse leaves it) -- next to this library's FP32/int32 and
+    FP16/packed-16 products of the same matrix (a tenth of the optimization
+    matrix's rows, still far larger than L2)."""
+    import torch
+
+    from fastdose_b200 import optimize
+
+    window, density = rows // 25, 0.5
+    s = torch.cuda.current_stream()
+
+    def timed(fn, reps=10):
+        for _ in range(3):
+            fn()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        for _ in range(reps):
+            fn()
+        e1.record(s)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    x = torch.rand(cols, device="cuda")
+    y = torch.empty(rows, device="cuda")
+    res = {"rows": rows, "cols": cols}
+    A, AT = optimize.Matrix.synthetic(ctx, rows, cols, window, density, seed=seed, value_type="f32", index_format="i32")
+    del AT
+    off, col, val = A.to_host()
+    res["nnz"] = int(len(val))
+    res["fd2_f32_i32_ms"] = timed(lambda: A.spmv(x, y, stream=s))
+    del A
+    S = torch.sparse_csr_tensor(torch.from_numpy(off).cuda(), torch.from_numpy(col.astype(np.int64)).cuda(),
+                                torch.from_numpy(val).cuda(), size=(rows, cols))
+    del off, col, val
+    xc = x.unsqueeze(1)
+    res["cusparse_f32_i64_ms"] = timed(lambda: torch.mm(S, xc))
+    ref_bytes = res["nnz"] * 12 + (rows + 1) * 8 + cols * 4 + rows * 4
+    res["cusparse_gbs"] = ref_bytes / res["cusparse_f32_i64_ms"] * 1e-6
+    del S, xc
+    A16, AT16 = optimize.Matrix.synthetic(ctx, rows, cols, window, density, seed=seed, value_type="f16",
+                                          index_format="packed16")
+    del AT16
+    res["fd2_f16_packed16_ms"] = timed(lambda: A16.spmv(x, y, stream=s))
+    res["f16_speedup_vs_cusparse_f32_i64"] = res["cusparse_f32_i64_ms"] / res["fd2_f16_packed16_ms"]
+    res["f32_speedup_vs_cusparse_f32_i64"] = res["cusparse_f32_i64_ms"] / res["fd2_f32_i32_ms"]
+    del A16
+    torch.cuda.empty_cache()
+    return res
 
 
 def served_requests(ctx, n_requests, seed=11):
