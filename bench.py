@@ -34,6 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "CCCS beamlets/s (dose-loading matrix, batched 4pi)"
+CCCS_DRAM_BYTES_PER_BEAMLET = 3.7612e9 / 610
 UNIT = "beamlets/s"
 
 
@@ -561,6 +562,10 @@ def run_fd2(args, rank, world):
     P = 16 * 16
     L = np.concatenate([b["long_dim"] for b in beamlets]).astype(np.float64)
     cccs_bytes = float(np.sum(4.0 * P * L * 3))  # Terma + density read, dose written, per beamlet
+    # DRAM bytes the CCCS kernel moves per beamlet: dram__bytes_read.sum + dram__bytes_write.sum of one
+    # ncu capture on the 4-beam plan (610 beamlets, 3.76 GB; profiles/cccs_kernel_4pi_torso_4beams.md),
+    # scaled by the beamlets of this step (each zenith pass re-reads its slices: traffic grows with beamlets)
+    cccs_traffic = CCCS_DRAM_BYTES_PER_BEAMLET * n_bl
     cccs_ms = stages["cccs"]
     peak, peak_kind = _peaks()
     achieved = cccs_bytes / (cccs_ms * 1e-3) / 1e9 if cccs_ms > 0 else None
@@ -576,7 +581,7 @@ def run_fd2(args, rank, world):
         "stage_ms_per_step": {k: v for k, v in stages.items() if v},
         "gpu_launches": int(launches),
         "roofline": {"bound": "hbm", "kernel": "cccs_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak if achieved else None, "traffic": None,
+                     "frac": achieved / peak if achieved else None, "traffic": cccs_traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_step": cccs_bytes},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "clocks": clk.summary(),
