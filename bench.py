@@ -198,6 +198,41 @@ class _DevView:
                                          "strides": None}
 
 
+def time_spmv(M, n_in, n_out, peak, reps=10, warmup=3):
+    """One product M x alone: CUDA-event time per launch after warm-up, and its
+    bandwidth (matrix stream + x + y) against the HBM peak."""
+    import torch
+
+    s = torch.cuda.current_stream()
+    xv = torch.rand(n_in, device="cuda")
+    yv = torch.empty(n_out, device="cuda")
+    for _ in range(warmup):
+        M.spmv(xv, yv, stream=s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        M.spmv(xv, yv, stream=s)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    nb = M.info()["device_bytes"] + n_in * 4 + n_out * 4  # matrix stream + x + y
+    return {"ms": ms, "bytes": nb, "gbs": nb / ms * 1e-6, "frac": nb / ms * 1e-6 / peak,
+            "x_in_shared": M.info()["x_in_shared"]}
+
+
+def spmv_leg(ctx, key, rows, seed=3, reps=10, warmup=3):
+    """--only-spmv: the optimization benchmark's synthetic pair (rows x 40k) in
+    one format, A x then A^T y timed alone (profiling)."""
+    from fastdose_b200 import optimize
+
+    vt, fmt = key.split("_")
+    cols = 40_000
+    A, AT = optimize.Matrix.synthetic(ctx, rows, cols, rows // 25, 0.5, seed=seed, value_type=vt, index_format=fmt)
+    peak, _ = _peaks()
+    return {"format": key, "rows": rows, "cols": cols, "nnz": A.info()["nnz"],
+            "A": time_spmv(A, cols, rows, peak, reps, warmup), "AT": time_spmv(AT, rows, cols, peak, reps, warmup)}
+
+
 def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
     """Fluence optimization on the IMRT-scale synthetic matrix: 2.5M VOI rows
     (PTV first) x 40k beamlets (400 beams x 10x10 maps), ~2% nonzeros, D from
@@ -236,26 +271,8 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
                              w["min_weights"], w["oar_weights"], 1.0, 0.1)
         bw = 0.1 * P.beam_weights_init(groups)
         # SpMV alone: A x and A^T y over the whole matrix
-        s = torch.cuda.current_stream()
-
-        def time_spmv(M, n_in, n_out, reps=10):
-            xv = torch.rand(n_in, device="cuda")
-            yv = torch.empty(n_out, device="cuda")
-            for _ in range(3):
-                M.spmv(xv, yv, stream=s)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(s)
-            for _ in range(reps):
-                M.spmv(xv, yv, stream=s)
-            e1.record(s)
-            torch.cuda.synchronize()
-            ms = e0.elapsed_time(e1) / reps
-            nb = M.info()["device_bytes"] + n_in * 4 + n_out * 4  # matrix stream + x + y
-            return {"ms": ms, "bytes": nb, "gbs": nb / ms * 1e-6, "frac": nb / ms * 1e-6 / peak,
-                    "x_in_shared": M.info()["x_in_shared"]}
-
-        spmv_a = time_spmv(A, cols, rows)
-        spmv_at = time_spmv(AT, rows, cols)
+        spmv_a = time_spmv(A, cols, rows, peak)
+        spmv_at = time_spmv(AT, rows, cols, peak)
         P.boo(groups, bw, x0, step_size=1e-3, iters=3, want=0, change_trigger=10 ** 9)  # warm-up
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -611,8 +628,20 @@ def main():
     ap.add_argument("--opt-iters", type=int, default=40)
     ap.add_argument("--opt-rows", type=int, default=2_500_000)
     ap.add_argument("--only-optimizer", action="store_true", help="run the optimizer leg alone (profiling)")
+    ap.add_argument("--only-spmv", default=None, choices=["f32_i32", "f32_packed16", "f16_packed16", "bf16_packed16"],
+                    help="time A x and A^T y of the optimization matrix in one format (profiling)")
+    ap.add_argument("--spmv-reps", type=int, default=10)
     ap.add_argument("--only-served", action="store_true", help="run the served leg alone")
     args = ap.parse_args()
+    if args.only_spmv:
+        import torch
+
+        from fastdose_b200 import api
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"spmv": spmv_leg(api.Context(0), args.only_spmv, args.opt_rows, reps=args.spmv_reps)}),
+              flush=True)
+        return
     if args.only_optimizer or args.only_served:
         import torch
 
