@@ -588,4 +588,147 @@ int fd2_polish(fd2_opt_problem* p, int iters_global, int iters_local, fd2_opt_st
     return solve(p, 0, nullptr, nullptr, 1, iters_global, iters_local, 0, st);
 }
 
+int fd2_beam_orientation_optimization(fd2_context* ctx, const fd2_matrix* AT, const fd2_matrix* D, int64_t n_beams,
+                                      const int64_t* h_beam_rows, const int64_t* h_d_rows, int64_t n_ptv,
+                                      int64_t n_oar, const float* h_max_dose, const float* h_max_weights,
+                                      const float* h_min_dose, const float* h_min_weights,
+                                      const float* h_oar_weights, const fd2_boo_params_t* prm, const float* d_x0,
+                                      float* h_costs, int32_t* h_active, float* h_norms, float* d_x,
+                                      fd2_boo_result_t* result) {
+    FD2_REQUIRE(ctx && AT && D && h_beam_rows && h_d_rows && prm && d_x0 && h_costs && h_active && h_norms && d_x &&
+                    result && n_beams > 0,
+                FD2_ERR_INVALID_ARGUMENT, "beam_orientation_optimization: bad argument");
+    FD2_REQUIRE(h_beam_rows[0] == 0 && h_beam_rows[n_beams] == AT->rows && h_d_rows[0] == 0 &&
+                    h_d_rows[n_beams] == D->rows && D->cols == AT->rows,
+                FD2_ERR_INVALID_ARGUMENT, "beam_orientation_optimization: beam blocks do not match AT (%lld rows) and D "
+                "(%lld x %lld)", (long long)AT->rows, (long long)D->rows, (long long)D->cols);
+    FD2_REQUIRE(prm->step_size > 0.0f && prm->max_iter > 0 && prm->change_weights_trigger > 0,
+                FD2_ERR_INVALID_ARGUMENT, "beam_orientation_optimization: bad parameters");
+    cudaStream_t s = ctx->stream;
+    const int64_t n_all = AT->rows;
+    // x and v of the active beams, ping-ponged through the reductions
+    float *xb[2] = {nullptr, nullptr}, *vb[2] = {nullptr, nullptr};
+    auto release = [&]() {
+        for (float* q : {xb[0], xb[1], vb[0], vb[1]})
+            if (q) cudaFree(q);
+    };
+    for (float** q : {&xb[0], &xb[1], &vb[0], &vb[1]})
+        if (cudaMalloc(q, std::max<int64_t>(n_all, 1) * sizeof(float)) != cudaSuccess) {
+            release();
+            set_error("beam_orientation_optimization: out of device memory");
+            return FD2_ERR_OUT_OF_MEMORY;
+        }
+    int cur = 0;
+    cudaError_t ce = cudaMemcpyAsync(xb[0], d_x0, n_all * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    if (ce == cudaSuccess) ce = cudaMemcpyAsync(vb[0], d_x0, n_all * sizeof(float), cudaMemcpyDeviceToDevice, s);
+    if (ce != cudaSuccess) {
+        release();
+        FD2_CHECK_CUDA(ce);
+    }
+    std::vector<int64_t> active(n_beams);
+    for (int64_t b = 0; b < n_beams; b++) active[b] = b;
+    std::vector<float> w;  // weights of the active beams, in order
+    fd2_opt_state_t st{};
+    st.k_global = 0;
+    st.theta_km1 = 0.0f;
+    st.tkm1 = prm->step_size;
+    *result = fd2_boo_result_t{};
+    std::vector<float> nrm;
+    int rc = FD2_OK;
+    for (;;) {
+        const int64_t na = (int64_t)active.size();
+        bool identity = na == n_beams;
+        for (int64_t j = 0; identity && j < na; j++) identity = active[j] == j;
+        // the active beams' matrices: the inputs themselves while every beam is
+        // active in its original order, else a selection
+        fd2_matrix *ATs = nullptr, *As = nullptr, *Ds = nullptr, *DTs = nullptr;
+        const fd2_matrix* ATp = AT;
+        const fd2_matrix* Dp = D;
+        if (!identity) {
+            rc = matrix_select_blocks(AT, n_beams, h_beam_rows, nullptr, na, active.data(), &ATs);
+            if (!rc) rc = matrix_select_blocks(D, n_beams, h_d_rows, h_beam_rows, na, active.data(), &Ds);
+            ATp = ATs;
+            Dp = Ds;
+        }
+        if (!rc) rc = matrix_transpose_fmt(ATp, ATp->index_format, &As);
+        if (!rc) rc = matrix_transpose_fmt(Dp, Dp->index_format, &DTs);
+        fd2_opt_problem* p = nullptr;
+        if (!rc)
+            rc = fd2_opt_problem_create(ctx, As, ATp, Dp, DTs, n_ptv, n_oar, h_max_dose, h_max_weights, h_min_dose,
+                                        h_min_weights, h_oar_weights, prm->gamma, prm->eta, &p);
+        std::vector<int64_t> go(na + 1, 0);
+        for (int64_t j = 0; j < na; j++) go[j + 1] = go[j] + h_beam_rows[active[j] + 1] - h_beam_rows[active[j]];
+        if (!rc && result->phases == 0) {  // beamWeightsInit_func over all beams, times beamWeight
+            w.assign(na, 0.0f);
+            rc = fd2_beam_weights_init(p, na, go.data(), w.data());
+            for (float& q : w) q *= prm->beam_weight;
+        }
+        nrm.assign(na, 0.0f);
+        if (!rc) {
+            st.d_xkm1 = xb[cur];
+            st.d_vkm1 = vb[cur];
+            st.h_loss = h_costs;
+            st.h_nrm = nrm.data();
+            rc = fd2_boo_l2onehalf(p, na, go.data(), w.data(), prm->show_trigger, prm->change_weights_trigger,
+                                   prm->max_iter, prm->prune_trigger, prm->n_prune, prm->n_beams_want, &st);
+            result->trials += st.trials;
+            result->phases += 1;
+        }
+        fd2_opt_problem_destroy(p);
+        for (fd2_matrix* q : {ATs, As, Ds, DTs})
+            if (q) fd2_matrix_destroy(q);
+        if (rc) break;
+        // DimReduction: rank by group norm, keep the strictly active beams
+        std::vector<int64_t> rank(na);
+        for (int64_t j = 0; j < na; j++) rank[j] = j;
+        std::stable_sort(rank.begin(), rank.end(), [&](int64_t a, int64_t b) { return nrm[a] > nrm[b]; });
+        const int64_t keep = std::min<int64_t>(na, std::max<int64_t>(0, (int64_t)st.num_active));
+        std::vector<int64_t> next(keep);
+        std::vector<float> w_next(keep), nrm_next(keep);
+        int64_t off = 0;
+        for (int64_t i = 0; i < keep && ce == cudaSuccess; i++) {
+            const int64_t j = rank[i];
+            next[i] = active[j];
+            w_next[i] = w[j];
+            nrm_next[i] = nrm[j];
+            const int64_t len = go[j + 1] - go[j];
+            if (len) {
+                ce = cudaMemcpyAsync(xb[cur ^ 1] + off, xb[cur] + go[j], len * sizeof(float), cudaMemcpyDeviceToDevice,
+                                     s);
+                if (ce == cudaSuccess)
+                    ce = cudaMemcpyAsync(vb[cur ^ 1] + off, vb[cur] + go[j], len * sizeof(float),
+                                         cudaMemcpyDeviceToDevice, s);
+            }
+            off += len;
+        }
+        if (ce != cudaSuccess) {
+            rc = FD2_ERR_CUDA;
+            set_error("beam_orientation_optimization: %s", cudaGetErrorString(ce));
+            break;
+        }
+        cur ^= 1;
+        active = next;
+        w = w_next;
+        nrm = nrm_next;
+        if (st.stop || keep == 0) {
+            for (int64_t i = 0; i < keep; i++) {
+                h_active[i] = (int32_t)active[i];
+                h_norms[i] = nrm[i];
+            }
+            result->n_active = (int32_t)keep;
+            result->iterations = st.k_global;
+            ce = cudaMemcpyAsync(d_x, xb[cur], off * sizeof(float), cudaMemcpyDeviceToDevice, s);
+            if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+            if (ce != cudaSuccess) {
+                rc = FD2_ERR_CUDA;
+                set_error("beam_orientation_optimization: %s", cudaGetErrorString(ce));
+            }
+            break;
+        }
+    }
+    cudaStreamSynchronize(s);
+    release();
+    return rc;
+}
+
 }  // extern "C"

@@ -91,6 +91,9 @@ int matrix_finalize(fd2_matrix* m, cudaStream_t stream);
 void matrix_free(fd2_matrix* m);
 // Transpose into a matrix of the given index format.
 int matrix_transpose_fmt(const fd2_matrix* m, int index_format, fd2_matrix** out);
+// Row blocks of m in a given order (fd2_matrix_select_blocks).
+int matrix_select_blocks(const fd2_matrix* m, int64_t n_blocks, const int64_t* h_rows, const int64_t* h_cols,
+                         int64_t n_keep, const int64_t* h_order, fd2_matrix** out);
 // y = M x on `stream`.  Not re-entrant per matrix: a column-scaled matrix
 // stages the scaled x, and every product its carries, in the matrix's buffers.
 int matrix_spmv(const fd2_matrix* m, const float* d_x, float* d_y, cudaStream_t stream);

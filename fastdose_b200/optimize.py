@@ -113,6 +113,18 @@ class Matrix:
         _lib.check(self.ctx.lib.fd2_matrix_transpose(self.h, C.byref(h)), "matrix_transpose")
         return Matrix(self.ctx, h)
 
+    def select_blocks(self, block_rows, order, block_cols=None):
+        """Row blocks `order` of this matrix, in that order (fd2_matrix_select_blocks);
+        with block_cols the columns are renumbered block by block (block-diagonal)."""
+        br = np.ascontiguousarray(block_rows, np.int64)
+        od = np.ascontiguousarray(order, np.int64)
+        bc = None if block_cols is None else np.ascontiguousarray(block_cols, np.int64)
+        h = C.c_void_p()
+        _lib.check(self.ctx.lib.fd2_matrix_select_blocks(self.h, len(br) - 1, _p(br), _p(bc) if bc is not None else None,
+                                                         len(od), _p(od) if od.size else None, C.byref(h)),
+                   "matrix_select_blocks")
+        return Matrix(self.ctx, h)
+
     def spmv(self, x, y=None, stream=None):
         torch = _torch()
         rows, _ = self.shape
@@ -246,6 +258,75 @@ class Problem:
             self.close()
         except Exception:
             pass
+
+
+def reference_x0(n, seed=10086):
+    """The reference's initial fluence for the beam-orientation loop:
+    std::srand(10086) then (float)std::rand() / RAND_MAX per beamlet
+    (IMRTOptimize.cu:240-243), with glibc's rand() restated -- the additive
+    feedback generator r[i] = r[i-3] + r[i-31] (mod 2^32) seeded through
+    16807 * r mod (2^31 - 1), whose first 344 outputs are discarded and which
+    returns r >> 1."""
+    r = [0] * (n + 344)
+    r[0] = seed & 0xFFFFFFFF
+    for i in range(1, 31):
+        hi, lo = divmod(int(np.int32(np.uint32(r[i - 1]))), 127773)
+        word = 16807 * lo - 2836 * hi
+        if word < 0:
+            word += 2147483647
+        r[i] = word
+    for i in range(31, 34):
+        r[i] = r[i - 31]
+    for i in range(34, n + 344):
+        r[i] = (r[i - 31] + r[i - 3]) & 0xFFFFFFFF
+    out = np.array([r[i] >> 1 for i in range(344, n + 344)], np.int64)
+    return (out.astype(np.float32) / np.float32(2147483647)).astype(np.float32)
+
+
+class _BooParams(C.Structure):
+    _fields_ = [("beam_weight", C.c_float), ("step_size", C.c_float), ("gamma", C.c_float), ("eta", C.c_float),
+                ("max_iter", C.c_int32), ("change_weights_trigger", C.c_int32), ("show_trigger", C.c_int32),
+                ("n_beams_want", C.c_int32), ("prune_trigger", C.c_void_p), ("n_prune", C.c_int32),
+                ("reserved", C.c_int32)]
+
+
+class _BooResult(C.Structure):
+    _fields_ = [("iterations", C.c_int32), ("n_active", C.c_int32), ("phases", C.c_int32), ("trials", C.c_int32)]
+
+
+def beam_orientation_optimization(ctx, AT, D, beam_rows, d_rows, n_ptv, n_oar, max_dose, max_weights, min_dose,
+                                  min_weights, oar_weights, x0, beam_weight=1.0, step_size=1e-3, gamma=1.0, eta=0.1,
+                                  max_iter=1000, change_weights_trigger=100, show_trigger=100, n_beams_want=20,
+                                  prune_trigger=()):
+    """IMRT::BeamOrientationOptimization with DimReduction, on the device.
+
+    AT: Matrix, beamlets x VOI rows of all candidate beams (beam b = rows
+    beam_rows[b]:beam_rows[b+1]); D: Matrix, the block-diagonal fluence
+    gradient (beam b = rows d_rows[b]:d_rows[b+1], its beamlets as columns);
+    x0: initial fluence of all beamlets.  Returns the kept beams in their final
+    order, their group norms and fluence, and the cost of every iteration."""
+    torch = _torch()
+    br = np.ascontiguousarray(beam_rows, np.int64)
+    dr = np.ascontiguousarray(d_rows, np.int64)
+    n_beams = len(br) - 1
+    arrs = [np.ascontiguousarray(a, np.float32) for a in (max_dose, max_weights, min_dose, min_weights, oar_weights)]
+    pr = np.ascontiguousarray(prune_trigger, np.int32)
+    prm = _BooParams(beam_weight, step_size, gamma, eta, max_iter, change_weights_trigger, show_trigger, n_beams_want,
+                     pr.ctypes.data if pr.size else None, pr.size, 0)
+    x0 = _dev_f32(x0)
+    x = torch.zeros_like(x0)
+    costs = np.zeros(max_iter, np.float32)
+    active = np.zeros(n_beams, np.int32)
+    norms = np.zeros(n_beams, np.float32)
+    res = _BooResult()
+    _join_torch()
+    _lib.check(ctx.lib.fd2_beam_orientation_optimization(
+        ctx.h, AT.h, D.h, n_beams, _p(br), _p(dr), n_ptv, n_oar, *(_p(a) for a in arrs), C.byref(prm), _ptr(x0),
+        _p(costs), _p(active), _p(norms), _ptr(x), C.byref(res)), "beam_orientation_optimization")
+    k = res.n_active
+    nx = int(sum(br[b + 1] - br[b] for b in active[:k]))
+    return dict(active=active[:k].copy(), norms=norms[:k].copy(), x=x[:nx], costs=costs[:min(res.iterations + 1, max_iter)],
+                costs_full=costs, iterations=res.iterations, phases=res.phases, trials=res.trials)
 
 
 def prox_l2onehalf(ctx, group_offsets, g0, tau, stream=None):

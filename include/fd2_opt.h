@@ -178,6 +178,68 @@ int fd2_boo_l2onehalf(fd2_opt_problem* p, int64_t n_groups, const int64_t* h_gro
 /* polish_BOO_IMRT_gpu */
 int fd2_polish(fd2_opt_problem* p, int iters_global, int iters_local, fd2_opt_state_t* st);
 
+/*
+ * Row-block selection (replaces parallelMatCoalesce over the active beams'
+ * VOIMatricesT and diagBlock over their SpFluenceGrad, IMRTOptimize.cu:278-300,
+ * IMRTEigenLoad.cpp:190-304, done on the host there at every prune phase):
+ * block b = rows [h_block_rows[b], h_block_rows[b+1]) of m; the blocks
+ * h_order[0..n_keep) are copied, in that order, into a new matrix of the same
+ * value type, index format and scale axis.  With h_block_cols (m block-
+ * diagonal: block b's rows use only columns [h_block_cols[b], h_block_cols[b+1]))
+ * the columns are renumbered block by block in the kept order; with NULL they
+ * are unchanged.  Values are copied, not re-rounded.
+ */
+int fd2_matrix_select_blocks(const fd2_matrix* m, int64_t n_blocks, const int64_t* h_block_rows,
+                             const int64_t* h_block_cols, int64_t n_keep, const int64_t* h_order, fd2_matrix** out);
+
+/* Parameters of the beam-orientation loop (the reference's Params). */
+typedef struct fd2_boo_params {
+    float beam_weight;             /* beamWeight: factor on the initial beam weights */
+    float step_size;               /* stepSize: initial step t */
+    float gamma, eta;              /* Huber threshold and TV weight */
+    int32_t max_iter;              /* maxIter: global iteration budget */
+    int32_t change_weights_trigger;
+    int32_t show_trigger;          /* the reference's progress print period (no output here) */
+    int32_t n_beams_want;          /* numBeamsWeWant */
+    const int32_t* prune_trigger;  /* pruneTrigger: ascending global iterations that end a phase */
+    int32_t n_prune;
+    int32_t reserved;
+} fd2_boo_params_t;
+
+typedef struct fd2_boo_result {
+    int32_t iterations;  /* k_global at the end */
+    int32_t n_active;    /* beams kept */
+    int32_t phases;      /* solver phases (matrix selections) run */
+    int32_t trials;      /* line-search trials over all phases */
+} fd2_boo_result_t;
+
+/*
+ * BeamOrientationOptimization (IMRTOptimize.cu:197-388) with DimReduction
+ * (IMRTOptUtils.cu:726-793), the matrices never leaving the device.
+ *   AT     beamlets x VOI rows of all candidate beams; beam b owns rows
+ *          [h_beam_rows[b], h_beam_rows[b+1]) (its active beamlets)
+ *   D      block-diagonal fluence-gradient operator; beam b owns rows
+ *          [h_d_rows[b], h_d_rows[b+1]) and columns [h_beam_rows[b], h_beam_rows[b+1])
+ *   VOI weights as fd2_opt_problem_create
+ *   d_x0   initial fluence of all beamlets (the reference draws rand()/RAND_MAX
+ *          after srand(10086), IMRTOptimize.cu:240-243); v starts equal to it
+ * Each phase runs the accelerated proximal-gradient loop until a prune trigger,
+ * the beam target or max_iter; then the beams are ranked by group norm
+ * (descending, ties by position) and those with norm > 1e-4 are kept, with
+ * their weights and their x, v segments, in that order.
+ * Out: h_costs[k] for every iteration k run ([max_iter]); h_active[0..n_active)
+ * the kept beams in their final order and h_norms their norms (the reference
+ * leaves its norms in the order before the last ranking); d_x[0..) the kept
+ * beams' fluence in that order (capacity: all beamlets).
+ */
+int fd2_beam_orientation_optimization(fd2_context* ctx, const fd2_matrix* AT, const fd2_matrix* D, int64_t n_beams,
+                                      const int64_t* h_beam_rows, const int64_t* h_d_rows, int64_t n_ptv,
+                                      int64_t n_oar, const float* h_max_dose, const float* h_max_weights,
+                                      const float* h_min_dose, const float* h_min_weights,
+                                      const float* h_oar_weights, const fd2_boo_params_t* params, const float* d_x0,
+                                      float* h_costs, int32_t* h_active, float* h_norms, float* d_x,
+                                      fd2_boo_result_t* result);
+
 #if defined(__GNUC__)
 #pragma GCC visibility pop
 #endif

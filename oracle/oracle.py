@@ -298,14 +298,17 @@ class Problem:
         return v, g
 
     def boo(self, group_offsets, beam_weights, x0, step_size, iters, prune=(), want=0,
-            change_trigger=100, show=100):
+            change_trigger=100, show=100, state=None, loss=None):
+        """state: (k_global, theta_km1, tkm1, v) carried from an earlier call;
+        loss: the [iters] cost array to fill at the iterations run."""
         go = np.ascontiguousarray(group_offsets, np.int64)
         w = _f32(beam_weights).copy()
         x = _f32(x0).copy()
-        v = x.copy()
-        loss = np.zeros(iters, np.float32)
+        v = x.copy() if state is None else _f32(state[3]).copy()
+        loss = np.zeros(iters, np.float32) if loss is None else loss
         nrm = np.zeros(len(go) - 1, np.float32)
-        st = _State(0, 0.0, step_size, _p(x), _p(v), _p(loss), _p(nrm), 0.0, 0, 0)
+        k0, th0, t0 = (0, 0.0, step_size) if state is None else state[:3]
+        st = _State(k0, th0, t0, _p(x), _p(v), _p(loss), _p(nrm), 0.0, 0, 0)
         pr = np.ascontiguousarray(prune, np.int32)
         self.L.or_boo_l2onehalf(C.byref(self.s), C.c_int64(len(go) - 1), _p(go), _p(w), C.c_int(show),
                                 C.c_int(change_trigger), C.c_int(iters), _p(pr), C.c_int(pr.size), C.c_int(want),

@@ -50,3 +50,21 @@ def test_oracle_t_hat_known_answers():
         f = lambda q: tau * np.sqrt(q * g) + 0.5 * (q - 1) ** 2 * nrm2  # noqa: E731
         grid = np.linspace(1e-3, 1.0, 20001)
         assert f(s) <= f(grid).min() + 1e-6
+
+
+def test_reference_x0_is_glibc_rand():
+    """The beam-orientation loop's initial fluence: srand(10086), then
+    (float)rand() / RAND_MAX, checked against this host's C library."""
+    import ctypes
+
+    import numpy as np
+
+    from fastdose_b200 import optimize
+
+    libc = ctypes.CDLL("libc.so.6")
+    libc.srand(10086)
+    ref = np.array([np.float32(libc.rand()) / np.float32(2147483647) for _ in range(2000)], np.float32)
+    np.testing.assert_array_equal(optimize.reference_x0(2000), ref)
+    libc.srand(7)
+    ref7 = np.array([np.float32(libc.rand()) / np.float32(2147483647) for _ in range(50)], np.float32)
+    np.testing.assert_array_equal(optimize.reference_x0(50, seed=7), ref7)
