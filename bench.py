@@ -262,6 +262,11 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
     out = {"workload": f"synthetic VOI matrix {rows}x{cols} (PTV {n_ptv}), window {window}, density {density}, "
                        f"D from {n_beams} 10x10 maps, gamma 1, eta 0.1, beam weight 0.1; BOO iterations"}
     x0 = torch.full((cols,), 0.01, dtype=torch.float32, device="cuda")
+    # the FP32 matrix and plan are kept to dose every format's plan exactly:
+    # DVHs of the PTV and OAR rows against the FP32-optimized plan's
+    A32 = x32 = dvh32 = None
+    structures = [np.arange(n_ptv), np.arange(n_ptv, rows)]
+    n_bins = 200
     for vt, fmt in (("f32", "i32"), ("f32", "packed16"), ("f16", "packed16"), ("bf16", "packed16")):
         key = f"{vt}_{fmt}"
         A, AT = optimize.Matrix.synthetic(ctx, rows, cols, window, density, seed=seed, value_type=vt,
@@ -282,8 +287,20 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
                    "nnz": info["nnz"], "matrix_bytes": info["device_bytes"],
                    "exception_chunks": info["exception_chunks"],
                    "spmv": spmv_a, "spmv_transpose": spmv_at}
-        del P, A, AT
+        if A32 is None:
+            A32, x32 = A, r["x"].clone()
+            dose32 = A32.spmv(x32)
+            width = float(dose32.max().item()) / (n_bins - 1)
+            _, dvh32 = optimize.dvh(ctx, dose32, structures, n_bins, width)
+            out[key]["dvh"] = {"bins": n_bins, "bin_width": width, "structures": ["PTV rows", "OAR rows"]}
+        else:
+            _, dvh_k = optimize.dvh(ctx, A32.spmv(r["x"]), structures, n_bins, width)
+            out[key]["dvh_max_abs_diff_vs_f32"] = float(np.abs(dvh_k - dvh32).max())
+        del P, AT
+        if A is not A32:
+            del A
         torch.cuda.empty_cache()
+    del A32, x32
     out["reference_form"] = reference_form_spmv(ctx, rows // 10, cols, seed, peak)
     base = out["f32_i32"]
     for key in ("f32_packed16", "f16_packed16", "bf16_packed16"):

@@ -329,6 +329,43 @@ def beam_orientation_optimization(ctx, AT, D, beam_rows, d_rows, n_ptv, n_oar, m
                 costs_full=costs, iterations=res.iterations, phases=res.phases, trials=res.trials)
 
 
+def final_dose(A_full, beam_rows, active, x):
+    """resultDoseCalc (IMRTOptimize.cu:604-625): the dose of the kept beams'
+    fluence x (concatenated in the order `active`) through the all-beam matrix
+    A_full (voxels x beamlets, beam b = columns beam_rows[b]:beam_rows[b+1]);
+    the pruned beams' beamlets carry zero fluence."""
+    torch = _torch()
+    br = np.asarray(beam_rows, np.int64)
+    x = _dev_f32(x)
+    full = torch.zeros(int(br[-1]), dtype=torch.float32, device=x.device)
+    o = 0
+    for b in np.asarray(active, np.int64):
+        n = int(br[b + 1] - br[b])
+        full[br[b]:br[b + 1]] = x[o:o + n]
+        o += n
+    assert o == x.numel(), "x does not match the kept beams"
+    return A_full.spmv(full)
+
+
+def dvh(ctx, dose, structures, n_bins, bin_width, stream=None):
+    """Cumulative DVHs (fd2_dvh): `structures` is a list of voxel-index arrays;
+    returns uint64 counts [n_structs, n_bins] of voxels receiving at least
+    k * bin_width, and the same as volume fractions."""
+    torch = _torch()
+    dose = _dev_f32(dose)
+    sizes = [len(s) for s in structures]
+    off = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    vox = torch.as_tensor(np.concatenate([np.asarray(s, np.int32) for s in structures]) if structures
+                          else np.zeros(0, np.int32)).to(dose.device)
+    out = torch.empty((len(structures), n_bins), dtype=torch.int64, device=dose.device)
+    _join_torch()
+    _lib.check(ctx.lib.fd2_dvh(ctx.h, _ptr(dose), dose.numel(), len(structures), _p(off), _ptr(vox), int(n_bins),
+                               float(bin_width), _ptr(out), _stream_ptr(stream)), "dvh")
+    counts = out.cpu().numpy().astype(np.uint64)
+    frac = counts / np.maximum(np.asarray(sizes, np.float64), 1.0)[:, None]
+    return counts, frac
+
+
 def prox_l2onehalf(ctx, group_offsets, g0, tau, stream=None):
     """proxL2Onehalf_QL_gpu::evaluate: (prox, new group norms) as tensors."""
     torch = _torch()

@@ -16,6 +16,9 @@
  *   proxL2Onehalf_QL_gpu::evaluate         IMRTOpt/src/IMRTOptimize_var1.cu:502-570
  *   BOO_IMRT_L2OneHalf_gpu_QL              IMRTOpt/src/IMRTOptimize.cu:16-194
  *   polish_BOO_IMRT_gpu                    IMRTOpt/src/IMRTOptimize.cu:391-476
+ *   BeamOrientationOptimization            IMRTOpt/src/IMRTOptimize.cu:197-388
+ *   DimReduction                           IMRTOpt/src/IMRTOptUtils.cu:726-793
+ *   DVH curves of doseAnalyze              IMRTOpt/src/doseAnalyze.py:53-62
  *
  * Matrices hold int64 row offsets, int32 column indices and FP32, FP16 or BF16
  * values; 16-bit values carry one FP32 scale per column (a matrix of VOI rows x
@@ -191,6 +194,19 @@ int fd2_polish(fd2_opt_problem* p, int iters_global, int iters_local, fd2_opt_st
  */
 int fd2_matrix_select_blocks(const fd2_matrix* m, int64_t n_blocks, const int64_t* h_block_rows,
                              const int64_t* h_block_cols, int64_t n_keep, const int64_t* h_order, fd2_matrix** out);
+
+/*
+ * Cumulative dose-volume histograms (the curve doseAnalyze.py:53-62 draws from
+ * sorted structure doses, binned): structure s owns the voxel indices
+ * d_voxels[h_struct_offsets[s] .. h_struct_offsets[s+1]) (host offsets;
+ * structures may overlap); voxel v falls in bin floor(d_dose[v] / bin_width)
+ * clamped to [0, n_bins); d_cumulative[s * n_bins + k] = voxels of s in bins
+ * >= k, i.e. receiving at least k * bin_width.  Voxel indices outside
+ * [0, n_voxels) are an error.  Synchronises the stream.
+ */
+int fd2_dvh(fd2_context* ctx, const float* d_dose, int64_t n_voxels, int64_t n_structs,
+            const int64_t* h_struct_offsets, const int32_t* d_voxels, int n_bins, float bin_width,
+            unsigned long long* d_cumulative, void* stream);
 
 /* Parameters of the beam-orientation loop (the reference's Params). */
 typedef struct fd2_boo_params {

@@ -152,3 +152,53 @@ def test_beam_orientation_matches_oracle(ctx):
     x = got["x"].cpu().numpy()
     assert x.shape == ref["x"].shape
     assert np.abs(x - ref["x"]).max() <= 1e-2 * max(np.abs(ref["x"]).max(), 1e-6)
+
+
+def _dvh_reference(dose, structures, n_bins, width):
+    """Binned cumulative DVH in numpy float32 (the same bin rule)."""
+    out = np.zeros((len(structures), n_bins), np.uint64)
+    for s, vox in enumerate(structures):
+        d = dose[np.asarray(vox, np.int64)].astype(np.float32)
+        q = np.floor(d / np.float32(width))
+        k = np.clip(q, 0, n_bins - 1).astype(np.int64)
+        counts = np.bincount(k, minlength=n_bins).astype(np.uint64)
+        out[s] = np.cumsum(counts[::-1])[::-1]
+    return out
+
+
+def test_dvh_counts_match_numpy(ctx):
+    rng = np.random.default_rng(4)
+    n = 300_000
+    dose = (rng.gamma(2.0, 0.6, n)).astype(np.float32)
+    dose[:100] = -0.5  # clamps to the first bin
+    dose[100:200] = 1e6  # clamps to the last
+    structures = [rng.choice(n, 50_000, replace=False), np.arange(0, n, 7), np.arange(10), np.zeros(0, np.int64),
+                  np.arange(n)]  # overlapping, tiny, empty, everything
+    counts, frac = optimize.dvh(ctx, dose, structures, n_bins=400, bin_width=0.01)
+    np.testing.assert_array_equal(counts, _dvh_reference(dose, structures, 400, 0.01))
+    assert frac[0, 0] == 1.0 and counts[3].sum() == 0
+    from fastdose_b200 import _lib
+
+    with pytest.raises(_lib.FD2Error):
+        optimize.dvh(ctx, dose, [np.array([0, n])], n_bins=10, bin_width=1.0)  # voxel n is outside the dose
+
+
+def test_final_dose_and_dvh_of_the_kept_beams(ctx):
+    """resultDoseCalc: the kept beams' fluence through the all-beam matrix equals
+    the product over the kept beams' columns alone; its DVHs per structure."""
+    import torch
+
+    A, D, beam_cols, d_rows, w, n_ptv, n_oar = _case()
+    Am = optimize.Matrix.from_csr(ctx, *_csr_tuple(A)[:3], A.shape[1])
+    active = [4, 0, 2]
+    rng = np.random.default_rng(9)
+    n_keep = int(sum(beam_cols[b + 1] - beam_cols[b] for b in active))
+    x = rng.random(n_keep).astype(np.float32)
+    dose = optimize.final_dose(Am, beam_cols, active, torch.from_numpy(x).cuda()).cpu().numpy()
+    cols = np.concatenate([np.arange(beam_cols[b], beam_cols[b + 1]) for b in active])
+    ref = A[:, cols].astype(np.float64) @ x.astype(np.float64)
+    bound = abs(A[:, cols]).astype(np.float64) @ np.abs(x.astype(np.float64))
+    assert np.all(np.abs(dose - ref) <= 2e-5 * bound + 1e-30)
+    structures = [np.arange(n_ptv), np.arange(n_ptv, n_ptv + n_oar)]
+    counts, frac = optimize.dvh(ctx, dose, structures, n_bins=200, bin_width=float(dose.max()) / 199)
+    np.testing.assert_array_equal(counts, _dvh_reference(dose, structures, 200, float(dose.max()) / 199))
