@@ -87,4 +87,34 @@ inline bool polish_BOO_IMRT_gpu(fd2_opt_problem* problem, int iters_global, int 
     return fd2_polish(problem, iters_global, iters_local, &state) != FD2_OK;
 }
 
+// BeamOrientationOptimization (IMRTOpt/src/IMRTOptimize.cu:197-388): the
+// per-beam VOIMatricesT / SpFluenceGrad lists become the all-beam device
+// matrices AT and D with their beam row blocks; the initial fluence is an
+// argument (the reference draws it from rand() after srand(10086)).  Outputs as
+// the reference's costs / activeBeams / activeNorms, plus the kept beams'
+// fluence on the device.
+inline bool BeamOrientationOptimization(fd2_context* ctx, const fd2_matrix* AT, const fd2_matrix* D,
+                                        const std::vector<int64_t>& beam_rows, const std::vector<int64_t>& d_rows,
+                                        int64_t n_ptv, int64_t n_oar, const std::vector<float>& maxDose,
+                                        const std::vector<float>& maxWeightsLong,
+                                        const std::vector<float>& minDoseTarget,
+                                        const std::vector<float>& minDoseTargetWeights,
+                                        const std::vector<float>& OARWeightsLong, const fd2_boo_params_t& params,
+                                        const float* d_x0, std::vector<float>& costs, std::vector<int>& activeBeams,
+                                        std::vector<float>& activeNorms, float* d_x) {
+    const size_t n_beams = beam_rows.size() - 1;
+    costs.assign(params.max_iter, 0.0f);
+    std::vector<int32_t> active(n_beams);
+    activeNorms.assign(n_beams, 0.0f);
+    fd2_boo_result_t res{};
+    if (fd2_beam_orientation_optimization(ctx, AT, D, (int64_t)n_beams, beam_rows.data(), d_rows.data(), n_ptv, n_oar,
+                                          maxDose.data(), maxWeightsLong.data(), minDoseTarget.data(),
+                                          minDoseTargetWeights.data(), OARWeightsLong.data(), &params, d_x0,
+                                          costs.data(), active.data(), activeNorms.data(), d_x, &res) != FD2_OK)
+        return true;
+    activeBeams.assign(active.begin(), active.begin() + res.n_active);
+    activeNorms.resize(res.n_active);
+    return false;
+}
+
 }  // namespace IMRT
