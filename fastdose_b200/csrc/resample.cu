@@ -208,8 +208,11 @@ __global__ void __launch_bounds__(kColThreads) column_count_kernel(const ColumnI
 // the beamlet's temporary segment; writes the row's nnz and max |value|.
 // Rows (y, z) of the box are taken kColThreads at a time in voxel order; their
 // admissible x intervals are concatenated by a scan, and the concatenation is
-// processed kColChunk voxels at a time: candidate test, order-preserving
-// compaction, values, compaction of the nonzeros.
+// tested kColChunk voxels at a time with an order-preserving compaction.  The
+// candidates gather in shared memory across chunks and row groups until at
+// least kColChunk wait; then all threads compute their values (a few per
+// thread, so the block barrier after them waits on a balanced share) and the
+// nonzeros are compacted in order into the segment.
 __global__ void __launch_bounds__(kColThreads) column_value_kernel(
     const ColumnInfo* __restrict__ infos, const float* const* __restrict__ dose, const uint64_t* __restrict__ cap_off,
     int32_t* __restrict__ tmp_col, float* __restrict__ tmp_val, uint32_t* __restrict__ row_nnz,
@@ -227,10 +230,39 @@ __global__ void __launch_bounds__(kColThreads) column_value_kernel(
     __shared__ typename RMax::TempStorage max_tmp;
     __shared__ uint32_t s_roff[kColThreads + 1];  // start of each row's interval in the concatenation
     __shared__ int s_rx[kColThreads];             // first x of the row's interval
-    __shared__ int s_cand[kColChunk];             // voxel index of this chunk's candidates, in order
-    __shared__ float s_val[kColChunk];
+    __shared__ int s_cand[2 * kColChunk];         // voxel index of the waiting candidates, in order
+    __shared__ float s_val[2 * kColChunk];
     uint32_t written = 0;  // uniform across the block
+    uint32_t pend = 0;     // candidates waiting in s_cand (uniform)
     float vmax = 0.0f;
+    // values of the waiting candidates, then their nonzeros in order
+    auto flush = [&]() {
+        for (uint32_t k = threadIdx.x; k < pend; k += kColThreads) {
+            const int v = s_cand[k];
+            const int x = v % nx, y = (v / nx) % ny, z = v / (nx * ny);
+            s_val[k] = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
+        }
+        __syncthreads();
+        const uint32_t per = (pend + kColThreads - 1) / kColThreads;  // a contiguous run per thread
+        const uint32_t k0 = min(pend, threadIdx.x * per), k1 = min(pend, k0 + per);
+        uint32_t nzc = 0;
+        for (uint32_t k = k0; k < k1; k++) nzc += s_val[k] != 0.0f;
+        uint32_t npos, n_nz;
+        Scan(scan_tmp).ExclusiveSum(nzc, npos, n_nz);
+        for (uint32_t k = k0; k < k1; k++) {
+            if (s_val[k] != 0.0f) {
+                if (written + npos < cap) {
+                    tmp_col[base + written + npos] = s_cand[k];
+                    tmp_val[base + written + npos] = s_val[k];
+                }
+                vmax = fmaxf(vmax, fabsf(s_val[k]));
+                npos++;
+            }
+        }
+        written += n_nz;
+        pend = 0;
+        __syncthreads();  // s_cand / s_val / scan_tmp reuse
+    };
     for (int r0w = 0; r0w < rows; r0w += kColThreads) {
         const int r = r0w + threadIdx.x;
         int xa = 0, xb = 0;
@@ -242,7 +274,7 @@ __global__ void __launch_bounds__(kColThreads) column_value_kernel(
         if (threadIdx.x == 0) s_roff[kColThreads] = total;
         __syncthreads();
         for (uint32_t f0 = 0; f0 < total; f0 += kColChunk) {
-            // 1. candidate test, kPerThread consecutive voxels per thread
+            // candidate test, kPerThread consecutive voxels per thread
             uint32_t flags = 0, cnt = 0;
             int vox[kPerThread];
 #pragma unroll
@@ -268,42 +300,15 @@ __global__ void __launch_bounds__(kColThreads) column_value_kernel(
             uint32_t pos, n_cand;
             Scan(scan_tmp).ExclusiveSum(cnt, pos, n_cand);
 #pragma unroll
-            for (int q = 0; q < kPerThread; q++)
-                if (flags & (1u << q)) s_cand[pos++] = vox[q];
+            for (int q = 0; q < kPerThread; q++)  // pend < kColChunk and n_cand <= kColChunk
+                if (flags & (1u << q)) s_cand[pend + pos++] = vox[q];
+            pend += n_cand;
             __syncthreads();
-            // 2. values of the candidates, spread over all threads
-            for (uint32_t k = threadIdx.x; k < n_cand; k += kColThreads) {
-                const int v = s_cand[k];
-                const int x = v % nx, y = (v / nx) % ny, z = v / (nx * ny);
-                s_val[k] = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
-            }
-            __syncthreads();
-            // 3. nonzeros in order into the row's segment
-            uint32_t nzc = 0;
-#pragma unroll
-            for (int q = 0; q < kPerThread; q++) {
-                const uint32_t k = threadIdx.x * kPerThread + q;
-                if (k < n_cand && s_val[k] != 0.0f) nzc++;
-            }
-            uint32_t npos, n_nz;
-            Scan(scan_tmp).ExclusiveSum(nzc, npos, n_nz);
-#pragma unroll
-            for (int q = 0; q < kPerThread; q++) {
-                const uint32_t k = threadIdx.x * kPerThread + q;
-                if (k < n_cand && s_val[k] != 0.0f) {
-                    if (written + npos < cap) {
-                        tmp_col[base + written + npos] = s_cand[k];
-                        tmp_val[base + written + npos] = s_val[k];
-                    }
-                    vmax = fmaxf(vmax, fabsf(s_val[k]));
-                    npos++;
-                }
-            }
-            written += n_nz;
-            __syncthreads();  // s_cand / s_val / scan_tmp reuse
+            if (pend >= (uint32_t)kColChunk) flush();
         }
         __syncthreads();  // s_roff / s_rx reuse
     }
+    if (pend) flush();
     float m = RMax(max_tmp).Reduce(vmax, cub::Max());
     if (threadIdx.x == 0) {
         row_nnz[blockIdx.x] = written;
