@@ -333,10 +333,12 @@ class MatCSREnsemble:
         _lib.check(self.ctx.lib.fd2_csr_ensemble_tofile(self.h, str(folder).encode()), "ensemble_tofile")
 
     @classmethod
-    def fromfile(cls, ctx, folder, n_cols):
+    def fromfile(cls, ctx, folder, n_cols, value_type="f32"):
+        """f32 reads the reference's valuesBuffer.bin; f16/bf16 read the sidecars
+        a 16-bit ensemble's tofile wrote."""
         h = C.c_void_p()
-        _lib.check(ctx.lib.fd2_csr_ensemble_fromfile(ctx.h, str(folder).encode(), n_cols, 0, C.byref(h)),
-                   "ensemble_fromfile")
+        _lib.check(ctx.lib.fd2_csr_ensemble_fromfile(ctx.h, str(folder).encode(), n_cols, VALUE_TYPES[value_type],
+                                                     C.byref(h)), "ensemble_fromfile")
         return cls(ctx, h)
 
     def close(self):

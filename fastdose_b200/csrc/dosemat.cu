@@ -556,6 +556,11 @@ static int write_file(const std::string& path, const void* data, size_t bytes) {
     return FD2_OK;
 }
 
+// 16-bit sidecar files beside the reference's layout (valuesBuffer.bin stays
+// float32 with the scales applied, for the reference's readers)
+static std::string sidecar_values(int vt) { return vt == FD2_VALUES_F16 ? "/valuesBuffer.f16.bin" : "/valuesBuffer.bf16.bin"; }
+static std::string sidecar_scales(int vt) { return vt == FD2_VALUES_F16 ? "/rowScales.f16.bin" : "/rowScales.bf16.bin"; }
+
 static int read_file(const std::string& path, std::vector<char>& out) {
     std::ifstream f(path, std::ios::binary | std::ios::ate);
     FD2_REQUIRE(f.is_open(), FD2_ERR_IO, "cannot open %s", path.c_str());
@@ -601,21 +606,43 @@ int fd2_csr_ensemble_tofile(const fd2_csr_ensemble* e, const char* folder) {
     std::vector<uint64_t> col64(col.begin(), col.end());
     FD2_TRY(write_file(dir + "/columnsBuffer.bin", col64.data(), col64.size() * 8));
     FD2_TRY(write_file(dir + "/valuesBuffer.bin", val.data(), val.size() * 4));
+    if (e->value_type != FD2_VALUES_F32) {
+        // sidecars of a 16-bit ensemble: its stored values and row scales, so that
+        // a 16-bit load reads half the value bytes and reproduces the same bits
+        std::vector<uint16_t> raw(e->nnz);
+        std::vector<float> scale(e->n_rows);
+        if (e->nnz) FD2_CHECK_CUDA(cudaMemcpy(raw.data(), e->d_val, e->nnz * 2, cudaMemcpyDeviceToHost));
+        if (e->n_rows) FD2_CHECK_CUDA(cudaMemcpy(scale.data(), e->d_scale, e->n_rows * 4, cudaMemcpyDeviceToHost));
+        FD2_TRY(write_file(dir + sidecar_values(e->value_type), raw.data(), raw.size() * 2));
+        FD2_TRY(write_file(dir + sidecar_scales(e->value_type), scale.data(), scale.size() * 4));
+    }
     return FD2_OK;
 }
 
 int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_cols, int value_type,
                               fd2_csr_ensemble** out) {
     FD2_REQUIRE(ctx && folder && out, FD2_ERR_INVALID_ARGUMENT, "fromfile: null argument");
-    FD2_REQUIRE(value_type == FD2_VALUES_F32, FD2_ERR_NOT_SUPPORTED, "fromfile: only F32 storage");
+    FD2_REQUIRE(value_type >= FD2_VALUES_F32 && value_type <= FD2_VALUES_BF16, FD2_ERR_INVALID_ARGUMENT,
+                "fromfile: value type %d", value_type);
     *out = nullptr;
     const std::string dir(folder);
-    std::vector<char> b_nrows, b_off, b_col, b_val, b_nnz;
+    const bool half = value_type != FD2_VALUES_F32;
+    std::vector<char> b_nrows, b_off, b_col, b_val, b_nnz, b_scale;
     FD2_TRY(read_file(dir + "/numRowsPerMat.bin", b_nrows));
     FD2_TRY(read_file(dir + "/NonZeroElements.bin", b_nnz));
     FD2_TRY(read_file(dir + "/offsetsBuffer.bin", b_off));
     FD2_TRY(read_file(dir + "/columnsBuffer.bin", b_col));
-    FD2_TRY(read_file(dir + "/valuesBuffer.bin", b_val));
+    if (half) {
+        // a 16-bit ensemble loads from the sidecars its tofile wrote; folders from
+        // the reference (float32 only) load as F32 and are rounded by the VOI step
+        FD2_REQUIRE(std::ifstream(dir + sidecar_values(value_type)).good(), FD2_ERR_NOT_SUPPORTED,
+                    "fromfile: %s has no %s sidecar; load F32 and restrict with a 16-bit value type", folder,
+                    sidecar_values(value_type).c_str() + 1);
+        FD2_TRY(read_file(dir + sidecar_values(value_type), b_val));
+        FD2_TRY(read_file(dir + sidecar_scales(value_type), b_scale));
+    } else {
+        FD2_TRY(read_file(dir + "/valuesBuffer.bin", b_val));
+    }
     const size_t nm = b_nrows.size() / 8;
     FD2_REQUIRE(b_nnz.size() / 8 == nm, FD2_ERR_IO, "fromfile: NonZeroElements.bin has %zu entries, expected %zu",
                 b_nnz.size() / 8, nm);
@@ -623,11 +650,12 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
     const uint64_t* off = (const uint64_t*)b_off.data();
     const uint64_t* mnnz = (const uint64_t*)b_nnz.data();
     const size_t nnz = b_col.size() / 8;
-    FD2_REQUIRE(b_val.size() / 4 == nnz, FD2_ERR_IO, "fromfile: values/columns size mismatch");
+    FD2_REQUIRE(b_val.size() / (half ? 2 : 4) == nnz, FD2_ERR_IO, "fromfile: values/columns size mismatch");
     uint64_t total_rows = 0, check = 0;
     for (size_t m = 0; m < nm; m++) { total_rows += nrows[m]; check += mnnz[m]; }
     FD2_REQUIRE(check == nnz, FD2_ERR_IO, "fromfile: nnz mismatch");
     FD2_REQUIRE(b_off.size() / 8 == total_rows + nm, FD2_ERR_IO, "fromfile: offsetsBuffer size mismatch");
+    FD2_REQUIRE(!half || b_scale.size() / 4 == total_rows, FD2_ERR_IO, "fromfile: row scales size mismatch");
     std::vector<int64_t> ro(total_rows + 1, 0);
     std::vector<uint64_t> mat_rows(1, 0);
     size_t ob = 0, r = 0;
@@ -660,8 +688,9 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
         cudaMemcpy(e->d_row_off, ro.data(), ro.size() * 8, cudaMemcpyHostToDevice);
         if (nnz) {
             cudaMemcpy(e->d_col, col.data(), nnz * 4, cudaMemcpyHostToDevice);
-            cudaMemcpy(e->d_val, b_val.data(), nnz * 4, cudaMemcpyHostToDevice);
+            cudaMemcpy(e->d_val, b_val.data(), nnz * (half ? 2 : 4), cudaMemcpyHostToDevice);
         }
+        if (half && total_rows) cudaMemcpy(e->d_scale, b_scale.data(), total_rows * 4, cudaMemcpyHostToDevice);
         e->n_rows = total_rows;
         e->nnz = e->nnz_bound = nnz;
         if (cudaDeviceSynchronize() != cudaSuccess) rc = FD2_ERR_CUDA;

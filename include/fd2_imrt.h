@@ -108,10 +108,17 @@ int fd2_csr_ensemble_to_host(const fd2_csr_ensemble* e, int64_t* row_offsets, in
  * CumuNumRowsPerMat.bin, OffsetBufferIdx.bin (uint64[n_mats] each),
  * offsetsBuffer.bin (uint64, per matrix n_rows+1 local offsets), columnsBuffer.bin
  * (uint64[nnz]) and valuesBuffer.bin (float32[nnz]) into `folder` (created).
+ * A 16-bit ensemble also writes its stored values and row scales as sidecars
+ * (valuesBuffer.f16.bin or .bf16.bin: uint16[nnz]; rowScales.f16.bin or
+ * .bf16.bin: float32[n_rows]); the reference's files are unchanged by them.
  */
 int fd2_csr_ensemble_tofile(const fd2_csr_ensemble* e, const char* folder);
 
-/* MatCSREnsemble::fromfile (IMRTSparseMatEns.cu:242-337) into a device ensemble. */
+/*
+ * MatCSREnsemble::fromfile (IMRTSparseMatEns.cu:242-337) into a device ensemble.
+ * value_type F32 reads valuesBuffer.bin; F16/BF16 read that type's sidecars
+ * (the exact stored values and scales) and refuse a folder without them.
+ */
 int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_cols,
                               int value_type, fd2_csr_ensemble** out);
 

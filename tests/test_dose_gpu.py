@@ -153,6 +153,34 @@ def test_half_precision_matrix(ctx, vt, rel):
         assert np.abs(a - b).max() <= rel * np.abs(b).max() * 1.01
 
 
+@pytest.mark.parametrize("vt", ["f16", "bf16"])
+def test_half_precision_file_round_trip(ctx, tmp_path, vt):
+    """A 16-bit ensemble written to a doseMatFolder: the reference's files hold
+    the decoded float32 values, the sidecars the stored bits; loading the
+    sidecars gives back the same ensemble bit for bit.  A folder without them
+    (the reference's own) is refused for a 16-bit load."""
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    half = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn, value_type=vt)
+    ro, col, val = half.to_host()
+    half.tofile(tmp_path / "m")
+    np.testing.assert_array_equal(np.fromfile(tmp_path / "m" / "valuesBuffer.bin", np.float32), val)
+    assert (tmp_path / "m" / f"valuesBuffer.{vt}.bin").stat().st_size == 2 * len(val)
+    back = api.MatCSREnsemble.fromfile(ctx, tmp_path / "m", case["phantom"].density.size, value_type=vt)
+    assert back.info()["value_type"] == half.info()["value_type"]
+    for a, b in zip(back.to_host(), (ro, col, val)):
+        np.testing.assert_array_equal(a, b)
+    f32 = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn)
+    f32.tofile(tmp_path / "r")
+    from fastdose_b200 import _lib
+
+    with pytest.raises(_lib.FD2Error) as e:
+        api.MatCSREnsemble.fromfile(ctx, tmp_path / "r", case["phantom"].density.size, value_type=vt)
+    assert "sidecar" in str(e.value)
+    for m in (half, back, f32):
+        m.close()
+
+
 def test_dose_matrix_c1_matches_oracle(ctx):
     """Whole config-1 plan (100 beamlets, 6 azimuths) against the FP64 oracle:
     the mean criterion of the parity gate; the maximum is bounded by the
