@@ -341,6 +341,14 @@ class MatCSREnsemble:
                                                      C.byref(h)), "ensemble_fromfile")
         return cls(ctx, h)
 
+    @classmethod
+    def concat(cls, ctx, parts):
+        """The matrices of several ensembles as one, in order (fd2_csr_ensemble_concat)."""
+        arr = (C.c_void_p * len(parts))(*[p.h for p in parts])
+        h = C.c_void_p()
+        _lib.check(ctx.lib.fd2_csr_ensemble_concat(ctx.h, len(parts), arr, C.byref(h)), "ensemble_concat")
+        return cls(ctx, h)
+
     def close(self):
         if self.h:
             self.ctx.lib.fd2_csr_ensemble_destroy(self.h)

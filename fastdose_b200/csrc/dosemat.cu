@@ -56,6 +56,20 @@ void rot_axis_d(const double p[3], const double r[3], double t, double o[3]) {
 // Grows the ensemble's device arrays (amortised growth), from the context's
 // pool and in the order of the ensemble's stream: the old contents are copied
 // and the old arrays freed asynchronously.
+__global__ void offsets_shift_kernel(const int64_t* __restrict__ src, uint64_t n, int64_t shift,
+                                     int64_t* __restrict__ dst) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[i] + shift;
+}
+
+// dst[i] = src[i] + shift for i < n (row offsets of a part moved after the parts before it)
+int launch_offsets_shift(const int64_t* src, uint64_t n, int64_t shift, int64_t* dst, cudaStream_t st) {
+    const unsigned blocks = (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, 148 * 8));
+    offsets_shift_kernel<<<blocks, 256, 0, st>>>(src, n, shift, dst);
+    FD2_CHECK_CUDA(cudaGetLastError());
+    return FD2_OK;
+}
+
 int ensemble_reserve(fd2_csr_ensemble* e, uint64_t rows, uint64_t nnz) {
     cudaStream_t st = e->stream;
     cudaMemPool_t pool = e->ctx->pool;
@@ -485,6 +499,64 @@ int fd2_bev2pvcs_interp(fd2_context* ctx, size_t n_beams, const uint32_t* n_per_
     }
     if (!rc) rc = ensemble_sync_nnz(e);
     if (rc) {
+        fd2_csr_ensemble_destroy(e);
+        return rc;
+    }
+    *out = e;
+    return FD2_OK;
+}
+
+int fd2_csr_ensemble_concat(fd2_context* ctx, size_t n, const fd2_csr_ensemble* const* parts,
+                            fd2_csr_ensemble** out) {
+    FD2_REQUIRE(ctx && parts && out && n > 0, FD2_ERR_INVALID_ARGUMENT, "ensemble_concat: bad argument");
+    uint64_t rows = 0, nnz = 0;
+    for (size_t i = 0; i < n; i++) {
+        FD2_REQUIRE(parts[i], FD2_ERR_INVALID_ARGUMENT, "ensemble_concat: part %zu is null", i);
+        FD2_REQUIRE(parts[i]->n_cols == parts[0]->n_cols && parts[i]->value_type == parts[0]->value_type,
+                    FD2_ERR_INVALID_ARGUMENT, "ensemble_concat: part %zu has another column count or value type", i);
+        rows += parts[i]->n_rows;
+        nnz += parts[i]->nnz;
+    }
+    *out = nullptr;
+    auto* e = new fd2_csr_ensemble();
+    e->ctx = ctx;
+    e->stream = ctx->stream;
+    e->n_cols = parts[0]->n_cols;
+    e->value_type = parts[0]->value_type;
+    e->mat_rows.assign(1, 0);
+    int rc = ensemble_reserve(e, rows, nnz);
+    cudaStream_t st = e->stream;
+    const size_t vb = value_bytes(e->value_type);
+    uint64_t r0 = 0, k0 = 0;
+    for (size_t i = 0; i < n && !rc; i++) {
+        const fd2_csr_ensemble* p = parts[i];
+        // the part's own stream has finished writing it
+        if (cudaStreamSynchronize(p->stream) != cudaSuccess) rc = FD2_ERR_CUDA;
+        if (!rc && p->n_rows) {
+            if (launch_offsets_shift(p->d_row_off + 1, p->n_rows, (int64_t)k0, e->d_row_off + r0 + 1, st) != FD2_OK)
+                rc = FD2_ERR_CUDA;
+            if (!rc && e->d_scale &&
+                cudaMemcpyAsync(e->d_scale + r0, p->d_scale, p->n_rows * sizeof(float), cudaMemcpyDeviceToDevice,
+                                st) != cudaSuccess)
+                rc = FD2_ERR_CUDA;
+        }
+        if (!rc && p->nnz &&
+            (cudaMemcpyAsync(e->d_col + k0, p->d_col, p->nnz * sizeof(int32_t), cudaMemcpyDeviceToDevice, st) !=
+                 cudaSuccess ||
+             cudaMemcpyAsync((char*)e->d_val + k0 * vb, p->d_val, p->nnz * vb, cudaMemcpyDeviceToDevice, st) !=
+                 cudaSuccess))
+            rc = FD2_ERR_CUDA;
+        for (size_t m = 1; m < p->mat_rows.size() && !rc; m++) e->mat_rows.push_back(r0 + p->mat_rows[m]);
+        r0 += p->n_rows;
+        k0 += p->nnz;
+    }
+    if (!rc) {
+        e->n_rows = rows;
+        e->nnz = e->nnz_bound = nnz;
+        if (cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    }
+    if (rc) {
+        if (rc == FD2_ERR_CUDA) set_error("ensemble_concat: %s", cudaGetErrorString(cudaGetLastError()));
         fd2_csr_ensemble_destroy(e);
         return rc;
     }

@@ -257,6 +257,29 @@ def config1():
                 long_spacing=0.25, extent=2.0)
 
 
+def config4(n_per_iso=300, dim=(256, 256, 200), seed=4, sub_fluence_dims=(12, 16, 20, 16)):
+    """Multi-isocentre head-and-neck plan: the head_neck_phantom's four PTV
+    segments, each with its own isocentre and n_per_iso candidate beams from
+    the 4pi sphere; per beam a fluence map of 6..20 beamlets a side (PTV
+    masking leaves 20-400 per beam); per isocentre its own BEV grid (sub-beam
+    map of sub_fluence_dims[k] pixels a side), so the plan is built as one
+    dose-loading matrix per isocentre."""
+    ph = head_neck_phantom(seed=seed, dim=dim)
+    rng = np.random.default_rng(seed + 100)
+    angles = sphere_beam_angles(n_per_iso)
+    isos = []
+    for k in range(4):
+        mask = ph.masks[f"PTVSeg{k}"]
+        # each isocentre sees the sphere from its own rotation of the couch axis
+        shift = rng.uniform(0.0, 2.0 * math.pi)
+        a = angles.copy()
+        a[:, 1] = ((a[:, 1] + shift + math.pi) % (2.0 * math.pi) - math.pi).astype(np.float32)
+        isos.append(dict(mask=mask, isocenter=mask_centroid(mask, ph.voxel), angles=a,
+                         fluence_dims=rng.integers(6, 21, size=len(a)), sub_fluence_dim=int(sub_fluence_dims[k])))
+    return dict(phantom=ph, spectrum=synthetic_spectrum(), kernel=synthetic_kernel(), isos=isos, beamlet_size=0.5,
+                sad=100.0, sub_fluence_on=4, long_spacing=0.25, extent=2.0)
+
+
 def config2(n_beams=400):
     """Batched 4pi CCCS: 200x200x160 torso, up to 400 candidate beams,
     16x16 beamlet grid of 0.5 cm, beamlets kept where they see the PTV."""

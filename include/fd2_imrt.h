@@ -124,6 +124,15 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
 
 int fd2_csr_ensemble_destroy(fd2_csr_ensemble* e);
 
+/*
+ * The matrices of several ensembles (same voxel count and value type) as one
+ * ensemble, in order, on ctx's stream -- e.g. the per-isocentre dose-loading
+ * matrices of a multi-isocentre plan for a joint optimization.  No reference
+ * counterpart (its joint problems concatenate the Eigen matrices on the host).
+ */
+int fd2_csr_ensemble_concat(fd2_context* ctx, size_t n, const fd2_csr_ensemble* const* parts,
+                            fd2_csr_ensemble** out);
+
 /* IMRT::beamletFlagSave (IMRTBeamBundle.cu:572-601): uint8 flags to a file. */
 int fd2_beamlet_flags_save(const uint8_t* flags, size_t n, const char* path);
 
