@@ -363,6 +363,103 @@ def reference_form_spmv(ctx, rows, cols, seed, peak):
     return res
 
 
+def c4_leg(ctx, n_per_iso=300, opt_iters=20):
+    """--c4: the multi-isocentre head-and-neck configuration -- 256x256x200 at
+    2.5 mm, four PTV segments with their own isocentres, n_per_iso beams each
+    (1200 in all) of 6..20 beamlets a side masked to the segment, one BEV grid
+    per isocentre (12, 16, 20, 16 pixels a side), one dose-loading matrix per
+    isocentre -- then the four matrices joined on the device and optimized
+    together with the FP16 matrix (PTV union rows and a subsampled ring)."""
+    import torch
+
+    from fastdose_b200 import api, optimize, phantoms
+    from fastdose_b200.types import make_bundle
+
+    cfg = phantoms.config4(n_per_iso)
+    ph = cfg["phantom"]
+    dens = api.Density(ctx, ph.density, ph.volume)
+    spec, kern = api.Spectrum(ctx, cfg["spectrum"]), api.Kernel(ctx, cfg["kernel"])
+    plans = []
+    for iso in cfg["isos"]:
+        bundles = np.array([make_bundle(iso["isocenter"], a, sad=cfg["sad"], fluence_dim=int(fd),
+                                        beamlet_size=cfg["beamlet_size"], sub_fluence_dim=iso["sub_fluence_dim"],
+                                        sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+                            for a, fd in zip(iso["angles"], iso["fluence_dims"])])
+        beams, flags, fds = [], [], []
+        for fd in np.unique(iso["fluence_dims"]):  # one flag pass per fluence dimension
+            idx = np.flatnonzero(iso["fluence_dims"] == fd)
+            for j, f in zip(idx, api.beamletFlagInit(ctx, bundles[idx], iso["mask"], ph.volume)):
+                b = api.bundle_beamlets(bundles[j], f, ph.volume)
+                if len(b):
+                    beams.append(b)
+                    flags.append(np.asarray(f).reshape(-1))
+                    fds.append(int(fd))
+        plans.append(dict(beams=beams, flags=flags, fds=fds, fluence=api.beamlet_fluence(bundles[0])))
+    n_beams = sum(len(p["beams"]) for p in plans)
+    n_bl = sum(len(b) for p in plans for b in p["beams"])
+    counts = [len(b) for p in plans for b in p["beams"]]
+    s = torch.cuda.current_stream()
+    # warm-up on a few beams of each grid, then the four matrices timed
+    for p in plans:
+        api.DoseMatConstruction(ctx, p["beams"][:2], p["fluence"], dens, spec, kern, stream=s).close()
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(plans) + 1)]
+    ev[0].record(s)
+    parts = []
+    for i, p in enumerate(plans):
+        parts.append(api.DoseMatConstruction(ctx, p["beams"], p["fluence"], dens, spec, kern, stream=s))
+        ev[i + 1].record(s)
+    torch.cuda.synchronize()
+    ms = ev[0].elapsed_time(ev[-1])
+    per_iso = [{"bev_grid": int(iso["sub_fluence_dim"]), "beamlets": int(sum(len(b) for b in p["beams"])),
+                "ms": ev[i].elapsed_time(ev[i + 1])} for i, (iso, p) in enumerate(zip(cfg["isos"], plans))]
+    for q in per_iso:
+        q["beamlets_per_s"] = q["beamlets"] / (q["ms"] * 1e-3)
+    joint = api.MatCSREnsemble.concat(ctx, parts)
+    nnz = joint.info()["nnz"]
+    for m in parts:
+        m.close()
+    # joint optimization, FP16 matrix
+    nv = ph.density.size
+    ptv = np.zeros(ph.density.shape, bool)
+    for iso in cfg["isos"]:
+        ptv |= iso["mask"].astype(bool)
+    ring = (ph.density > 0.5) & ~ptv
+    ptv_idx = np.flatnonzero(ptv.reshape(-1))
+    ring_idx = np.flatnonzero(ring.reshape(-1))[::8]
+    voxel_row = np.full(nv, -1, np.int32)
+    voxel_row[ptv_idx] = np.arange(len(ptv_idx))
+    voxel_row[ring_idx] = len(ptv_idx) + np.arange(len(ring_idx))
+    n_ptv, n_oar = len(ptv_idx), len(ring_idx)
+    t0 = time.perf_counter()
+    A, AT = optimize.Matrix.voi(ctx, joint, voxel_row, n_ptv + n_oar, value_type="f16", index_format="packed16")
+    torch.cuda.synchronize()
+    voi_s = time.perf_counter() - t0
+    joint.close()
+    D = optimize.block_diag([optimize.fluence_grad(fd, f) for p in plans for fd, f in zip(p["fds"], p["flags"])])
+    Dm = optimize.Matrix.from_csr(ctx, *D[:3], D[3])
+    P = optimize.Problem(ctx, A, AT, Dm, Dm.transpose(), n_ptv, n_oar, np.full(n_ptv + n_oar, 1.1, np.float32),
+                         np.ones(n_ptv + n_oar, np.float32), np.ones(n_ptv, np.float32), np.ones(n_ptv, np.float32),
+                         np.full(n_oar, 0.05, np.float32), 1.0, 0.1)
+    groups = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    bw = 0.1 * P.beam_weights_init(groups)
+    x0 = np.full(A.shape[1], 0.01, np.float32)
+    P.boo(groups, bw, x0, step_size=1e-3, iters=2, want=0, change_trigger=10 ** 9)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = P.boo(groups, bw, x0, step_size=1e-3, iters=opt_iters, want=0, change_trigger=10 ** 9)
+    opt_s = time.perf_counter() - t0
+    out = {"workload": f"multi-isocentre head and neck 256x256x200 @2.5mm, 4 isocentres, {n_beams} beams "
+                       f"({min(counts)}-{max(counts)} beamlets), BEV grids 12/16/20/16, 8x6 cones",
+           "beams": n_beams, "beamlets": n_bl, "nnz": int(nnz), "construction_ms": ms, "per_isocentre": per_iso,
+           "beamlets_per_s": n_bl / (ms * 1e-3), "voi_rows": n_ptv + n_oar, "voi_nnz": A.info()["nnz"],
+           "voi_restriction_s": voi_s, "opt_f16_it_per_s": r["k"] / opt_s,
+           "opt_loss_first_last": [float(r["loss"][0]), float(r["loss"][r["k"] - 1])]}
+    del P, A, AT, Dm
+    torch.cuda.empty_cache()
+    return out
+
+
 def served_requests(ctx, n_requests, seed=11):
     """Seeded plan requests of the served benchmark: a torso phantom whose
     sides are drawn from 96..256 voxels (2.5 mm), 1..50 beams from the 4pi
@@ -654,8 +751,17 @@ def main():
                     help="time A x and A^T y of the optimization matrix in one format (profiling)")
     ap.add_argument("--spmv-reps", type=int, default=10)
     ap.add_argument("--served-workers", type=int, default=2)
+    ap.add_argument("--c4", action="store_true", help="run the multi-isocentre configuration alone")
     ap.add_argument("--only-served", action="store_true", help="run the served leg alone")
     args = ap.parse_args()
+    if args.c4:
+        import torch
+
+        from fastdose_b200 import api
+
+        torch.cuda.set_device(0)
+        print(json.dumps({"c4": c4_leg(api.Context(0))}), flush=True)
+        return
     if args.only_spmv:
         import torch
 

@@ -77,11 +77,25 @@ __device__ __forceinline__ bool next_point(float3 c, float3 d, float3& np) {
 }
 
 // Lateral voxel column of the segment midpoint (d_calcCoords, DoseComp.cu:147-164).
+//
+// The reference's r = fmodf(m, ff), plus ff when negative, is computed
+// without fmodf: q = floor(m / ff) (the division may round q one off near a
+// multiple of ff), r = m - q ff in one fused operation, then one correction by
+// +-ff.  For m >= 0 the fused result is exact (the true remainder, or it minus
+// or plus ff, all representable by Sterbenz's lemma) and the correction lands
+// on the exact remainder, which is what fmodf returns.  For m < 0 the
+// reference rounds fmod + ff once; the fused operation rounds the same exact
+// value once, or, when q is one off, produces the exact fmod (Sterbenz) and the
+// correction rounds fmod + ff once.  Both paths give the reference's float.
 __device__ __forceinline__ int mid_index(float b, float n, float ff, int f) {
-    float m = __fmul_rn(__fadd_rn(b, n), 0.5f);
-    float r = fmodf(m, ff);
-    r = r < 0.0f ? __fadd_rn(r, ff) : r;
-    int i = (int)floorf(r);
+    const float m = __fmul_rn(__fadd_rn(b, n), 0.5f);
+    const float q = floorf(__fdiv_rn(m, ff));
+    float r = __fmaf_rn(-q, ff, m);
+    if (r < 0.0f)
+        r = __fadd_rn(r, ff);
+    else if (r >= ff)
+        r = __fsub_rn(r, ff);
+    const int i = (int)floorf(r);
     return i < f ? i : f - 1;
 }
 
@@ -124,8 +138,13 @@ __device__ __forceinline__ float seg_length(float l2) {
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
 // the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
 // sums).  RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
-template <int RPL, bool kFx16>
-__global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) cccs_kernel(const fd2_beam_t* __restrict__ beams,
+// kCols: every map of the batch is F x F with F <= 32 -- each lane owns one
+// column (lane % F) and the rows lane / F + k j (k = 32 / F lanes per column),
+// so the x half of the voxel work is done once per lane and the y half once per
+// row and shared by shuffles, as for 16 x 16 maps; RPL >= ceil(F / k).
+template <int RPL, bool kFx16, bool kCols = false>
+__global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || (kCols && RPL <= 8) ? 4 : (kCols ? 3 : 1))
+    cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
                                                    float* const* __restrict__ dose,
@@ -170,13 +189,21 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
     // per-ray constant pixel coordinates
     float fix[RPL], fiy[RPL];
     bool act[RPL];
+    if constexpr (!kFx16 && !kCols) {
 #pragma unroll
-    for (int j = 0; j < RPL; j++) {
-        int r = j * 32 + lane;
-        act[j] = r < g.P;
-        fix[j] = (float)(r % g.fx);
-        fiy[j] = (float)(r / g.fx);
+        for (int j = 0; j < RPL; j++) {
+            int r = j * 32 + lane;
+            act[j] = r < g.P;
+            fix[j] = (float)(r % g.fx);
+            fiy[j] = (float)(r / g.fx);
+        }
     }
+    // kCols: this lane's column and first row, the lanes per column, and the
+    // row whose y half this lane computes for the others
+    const int kgrp = kCols ? 32 / g.fx : 1;
+    const int ccol = kCols ? lane % g.fx : 0, cgrp = kCols ? lane / g.fx : 0;
+    const bool clane = kCols && lane < kgrp * g.fx;
+    const float fcol = (float)ccol, frow = (float)(kCols && lane < g.fy ? lane : 0);
 
     // register prefetch of the next slice's Terma/density (one pixel per thread)
     const bool prefetch = g.P <= (int)blockDim.x;
@@ -264,6 +291,38 @@ __global__ void __launch_bounds__(kFx16 ? kFx16Threads : 768, kFx16 ? 4 : 1) ccc
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
                     }
+                } else if constexpr (kCols) {
+                    const float btx = __fadd_rn(c.x, fcol), ntx = __fadd_rn(np.x, fcol);
+                    const int cx = mid_index(btx, ntx, g.ffx, g.fx);
+                    const bool wrapx = crosses_edge(btx, ntx, g.ffx);
+                    const float dxp = (ntx - g.hx) * g.bsx * fe - (btx - g.hx) * g.bsx * fs;
+                    const float dxz2 = dxp * dxp + dzp * dzp;
+                    const float bty = __fadd_rn(c.y, frow), nty = __fadd_rn(np.y, frow);
+                    const int ycode = mid_index(bty, nty, g.ffy, g.fy) | (crosses_edge(bty, nty, g.ffy) ? 64 : 0);
+                    const float dyq = (nty - g.hy) * g.bsy * fe - (bty - g.hy) * g.bsy * fs;
+#pragma unroll
+                    for (int j = 0; j < RPL; j++) {
+                        const int y = cgrp + kgrp * j;
+                        const bool on = clane && y < g.fy;
+                        const int yc = __shfl_sync(0xffffffffu, ycode, on ? y : 0);
+                        const float dyp = __shfl_sync(0xffffffffu, dyq, on ? y : 0);
+                        const int mi = on ? cx + g.fx * (yc & 63) : 0;
+                        const bool wrap = wrapx || (yc & 64);
+                        const float l2 = dxz2 + dyp * dyp;
+                        const float len = seg_length(l2);
+                        const float2 trv = tr[mi];
+                        const float p = len * trv.y;
+                        const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
+                        const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
+                        if (on) {
+                            float2 acc = mydp[mi];
+                            acc.x += dep;
+                            acc.y += p;
+                            mydp[mi] = acc;
+                        }
+                        XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
+                        XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
+                    }
                 } else {
 #pragma unroll
                 for (int j = 0; j < RPL; j++) {
@@ -347,6 +406,59 @@ __global__ void cccs_split_reduce(const fd2_beam_t* __restrict__ beams, float* c
     }
 }
 
+template <int RPL, bool kFx16, bool kCols>
+int launch_instance(unsigned blocks, int threads, size_t shm, cudaStream_t st, const fd2_beam_t* d_beams,
+                    const float* const* T, const float* const* R, float* const* D, const float4* dirs,
+                    const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status) {
+    FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<RPL, kFx16, kCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)shm));
+    cccs_kernel<RPL, kFx16, kCols><<<blocks, threads, shm, st>>>(d_beams, T, R, D, dirs, cp, split, planes,
+                                                                 plane_stride, status);
+    FD2_CHECK_CUDA(cudaGetLastError());
+    return FD2_OK;
+}
+
+// The march for a batch.  map: the common map side F when every map of the
+// batch is F x F, else 0.  16 x 16 maps take the 16-pixel instance; other
+// common sides up to 32 the shared-column instance (both need 4..8 azimuth
+// warps); anything else the general per-ray instance.
+int launch_march(int map, int maxP, int n_phi, unsigned blocks, cudaStream_t st, const fd2_beam_t* d_beams,
+                 const float* const* T, const float* const* R, float* const* D, const float4* dirs,
+                 const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status) {
+    const int threads = 32 * n_phi;
+    const size_t shm = (size_t)(1 + n_phi) * maxP * sizeof(float2);
+    const bool warps_ok = threads >= 128 && threads <= kFx16Threads;
+    if (map == 16 && threads <= kFx16Threads)
+        return launch_instance<8, true, false>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
+                                               plane_stride, status);
+    if (map > 0 && map <= 32 && warps_ok) {
+        const int k = 32 / map, rows = (map + k - 1) / k;  // rows per lane
+        if (rows <= 8)
+            return launch_instance<8, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                   planes, plane_stride, status);
+        if (rows <= 20)
+            return launch_instance<20, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                    planes, plane_stride, status);
+        if (rows <= 24)
+            return launch_instance<24, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                    planes, plane_stride, status);
+        return launch_instance<32, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
+                                                plane_stride, status);
+    }
+    if (maxP <= 256)
+        return launch_instance<8, false, false>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
+                                                plane_stride, status);
+    return launch_instance<32, false, false>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
+                                             plane_stride, status);
+}
+
+// common map side of a batch (F when every map is F x F), else 0
+int common_map(int side, const fd2_beam_t& b) {
+    const int fx = (int)b.fmap_size[0], fy = (int)b.fmap_size[1];
+    if (fx != fy) return 0;
+    return side < 0 ? fx : (side == fx ? side : 0);
+}
+
 }  // namespace
 
 int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams, const fd2_beam_t* d_beams,
@@ -391,29 +503,11 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     FD2_TRY(launch_cone_dirs(d_beams, n_beams, ang, d_dirs, stream));
     // slices a zenith pass skips must contribute zero
     if (plane_bytes) FD2_CHECK_CUDA(cudaMemsetAsync(d_planes, 0, plane_bytes, stream));
-    const int threads = 32 * k->n_phi;
-    const size_t shm = (size_t)(1 + k->n_phi) * maxP * sizeof(float2);
     const unsigned blocks = (unsigned)(schedule == 1 ? n_beams * fwd.size() : n_beams);
-    bool all16 = true;
-    for (size_t i = 0; i < n_beams && all16; i++) all16 = h_beams[i].fmap_size[0] == 16 && h_beams[i].fmap_size[1] == 16;
-    all16 = all16 && threads <= kFx16Threads;
-    if (all16) {
-        FD2_CHECK_CUDA(
-            cudaFuncSetAttribute(cccs_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<8, true><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
-                                                               d_planes, plane_stride, ctx->d_status);
-    } else if (maxP <= 256) {
-        FD2_CHECK_CUDA(
-            cudaFuncSetAttribute(cccs_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<8, false><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp,
-                                                                schedule, d_planes, plane_stride, ctx->d_status);
-    } else {
-        FD2_CHECK_CUDA(
-            cudaFuncSetAttribute(cccs_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<32, false><<<blocks, threads, shm, stream>>>(d_beams, d_terma, d_dens, d_dose, d_dirs, cp,
-                                                                 schedule, d_planes, plane_stride, ctx->d_status);
-    }
-    FD2_CHECK_CUDA(cudaGetLastError());
+    int map = -1;
+    for (size_t i = 0; i < n_beams && map != 0; i++) map = common_map(map, h_beams[i]);
+    FD2_TRY(launch_march(map, maxP, k->n_phi, blocks, stream, d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
+                         d_planes, plane_stride, ctx->d_status));
     ctx->launches += 2;  // direction table + march
     if (schedule == 1) {
         dim3 grid(std::max(1, std::min(64, (int)((plane_stride + 255) / 256))), (unsigned)n_beams);
@@ -576,7 +670,7 @@ extern "C" int fd2_dose_compute_static(size_t fmap_npixels, size_t n_beams, cons
     cudaStream_t st = (cudaStream_t)stream;
     fd2_beam_t hb[kBeamChunk];
     int maxP = 0;
-    bool all16 = true;
+    int map = -1;
     for (size_t i0 = 0; i0 < n_beams; i0 += kBeamChunk) {
         const size_t m = std::min(kBeamChunk, n_beams - i0);
         FD2_CHECK_CUDA(cudaMemcpyAsync(hb, d_beams + i0, m * sizeof(fd2_beam_t), cudaMemcpyDeviceToHost, st));
@@ -585,7 +679,7 @@ extern "C" int fd2_dose_compute_static(size_t fmap_npixels, size_t n_beams, cons
             FD2_REQUIRE(hb[i].TermaBEV_pitch == hb[i].DensityBEV_pitch, FD2_ERR_INVALID_ARGUMENT,
                         "dose_compute_static: Terma and density pitches differ");
             maxP = std::max(maxP, (int)(hb[i].fmap_size[0] * hb[i].fmap_size[1]));
-            all16 = all16 && hb[i].fmap_size[0] == 16 && hb[i].fmap_size[1] == 16;
+            map = map == 0 ? 0 : common_map(map, hb[i]);
         }
     }
     FD2_REQUIRE(maxP > 0 && maxP <= 1024, FD2_ERR_INVALID_ARGUMENT,
@@ -597,27 +691,10 @@ extern "C" int fd2_dose_compute_static(size_t fmap_npixels, size_t n_beams, cons
     float4* d_dirs = (float4*)(base + kStaticStatusBytes);
     FD2_CHECK_CUDA(cudaMemsetAsync(d_status, 0, sizeof(DeviceStatus), st));
     FD2_TRY(launch_cone_dirs(d_beams, n_beams, ang, d_dirs, st));
-    const int threads = 32 * cp.n_phi;
-    const size_t shm = (size_t)(1 + cp.n_phi) * maxP * sizeof(float2);
-    const unsigned blocks = (unsigned)n_beams;
     const float* const* T = (const float* const*)d_terma;
     const float* const* R = (const float* const*)d_density_bev;
-    if (all16 && threads <= kFx16Threads) {
-        FD2_CHECK_CUDA(
-            cudaFuncSetAttribute(cccs_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<8, true><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0, d_status);
-    } else if (maxP <= 256) {
-        FD2_CHECK_CUDA(
-            cudaFuncSetAttribute(cccs_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<8, false><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0,
-                                                            d_status);
-    } else {
-        FD2_CHECK_CUDA(
-            cudaFuncSetAttribute(cccs_kernel<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm));
-        cccs_kernel<32, false><<<blocks, threads, shm, st>>>(d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0,
-                                                             d_status);
-    }
-    FD2_CHECK_CUDA(cudaGetLastError());
+    FD2_TRY(launch_march(map, maxP, cp.n_phi, (unsigned)n_beams, st, d_beams, T, R, d_dose, d_dirs, cp, 0, nullptr, 0,
+                         d_status));
     if (status_out)
         FD2_CHECK_CUDA(cudaMemcpyAsync(status_out, &d_status->code, sizeof(int), cudaMemcpyDefault, st));
     return FD2_OK;
