@@ -716,6 +716,8 @@ def run_fd2(args, rank, world):
                    "parallelism": f"beams partitioned over {world} GPU(s), no collective"},
         "stage_ms_per_step": {k: v for k, v in stages.items() if v},
         "gpu_launches": int(launches),
+        "cccs_tuned": {"schedules": {str(k): v for k, v in ctx.tuned_schedules()[0].items()},
+                       "tuning_runs": ctx.tuned_schedules()[1]},
         "roofline": {"bound": "hbm", "kernel": "cccs_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": cccs_traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_step": cccs_bytes},

@@ -81,6 +81,16 @@ class Context:
 
     STAGES = ("terma", "cccs", "columns", "opt_spmv", "opt_other")
 
+    def tuned_schedules(self):
+        """The CCCS schedules the construction tuned: ({shape key: schedule}, tuning runs)."""
+        cap = 256
+        keys = (C.c_uint64 * cap)()
+        sch = (C.c_int32 * cap)()
+        n, runs = C.c_size_t(0), C.c_uint64(0)
+        _lib.check(self.lib.fd2_context_tuned_schedules(self.h, cap, keys, sch, C.byref(n), C.byref(runs)),
+                   "tuned_schedules")
+        return {int(keys[i]): int(sch[i]) for i in range(min(n.value, cap))}, int(runs.value)
+
     def set_timing(self, on=True):
         _lib.check(self.lib.fd2_context_set_timing(self.h, int(on)), "set_timing")
 
@@ -116,10 +126,14 @@ class Density:
         _lib.check(ctx.lib.fd2_density_create(ctx.h, _p(d), _p(self.volume), C.byref(h)), "density_create")
         self.h = h
 
+    def close(self):
+        if self.h:
+            self.ctx.lib.fd2_density_destroy(self.h)
+            self.h = None
+
     def __del__(self):
         try:
-            if self.h:
-                self.ctx.lib.fd2_density_destroy(self.h)
+            self.close()
         except Exception:
             pass
 
@@ -137,9 +151,14 @@ class Spectrum:
                    "spectrum_create")
         self.h = h
 
+    def close(self):
+        if self.h:
+            self.ctx.lib.fd2_spectrum_destroy(self.h)
+            self.h = None
+
     def __del__(self):
         try:
-            self.ctx.lib.fd2_spectrum_destroy(self.h)
+            self.close()
         except Exception:
             pass
 
@@ -157,9 +176,14 @@ class Kernel:
                                              C.byref(h)), "kernel_create")
         self.h = h
 
+    def close(self):
+        if self.h:
+            self.ctx.lib.fd2_kernel_destroy(self.h)
+            self.h = None
+
     def __del__(self):
         try:
-            self.ctx.lib.fd2_kernel_destroy(self.h)
+            self.close()
         except Exception:
             pass
 

@@ -96,6 +96,23 @@ int fd2_context_stage_times(fd2_context* c, double* ms, int n) {
 
 uint64_t fd2_context_launch_count(const fd2_context* c) { return c ? c->launches : 0; }
 
+int fd2_context_tuned_schedules(const fd2_context* c, size_t cap, uint64_t* keys, int32_t* schedules, size_t* n,
+                                uint64_t* runs) {
+    FD2_REQUIRE(c && n && runs && (cap == 0 || (keys && schedules)), FD2_ERR_INVALID_ARGUMENT,
+                "tuned_schedules: bad argument");
+    size_t i = 0;
+    for (const auto& kv : c->cccs_schedule) {
+        if (i < cap) {
+            keys[i] = kv.first;
+            schedules[i] = kv.second;
+        }
+        i++;
+    }
+    *n = i;
+    *runs = c->tuning_runs;
+    return FD2_OK;
+}
+
 int fd2_density_create(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume, fd2_density** out) {
     FD2_REQUIRE(ctx && host_density && volume && out, FD2_ERR_INVALID_ARGUMENT, "density_create: null argument");
     size_t nv = (size_t)volume->dim[0] * volume->dim[1] * volume->dim[2];

@@ -14,6 +14,7 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <numeric>
 #include <string>
 #include <sys/stat.h>
@@ -176,6 +177,44 @@ void make_column_info(const fd2_beam_t& b, const fd2_volume_t* vol, ColumnInfo& 
         ci.box[r] = (int)i0;
         ci.box[3 + r] = (int)i1;
     }
+}
+
+// The CCCS march of a batch under the context's tuned schedule.  Batches are
+// keyed by shape (beamlets to the nearest power of two, map pixels, cone
+// counts); the first batch of a shape runs both schedules -- one block per
+// beamlet over all zenith bins, and one block per (beamlet, zenith bin) -- and
+// keeps the faster for the shape.  The two give bitwise identical doses, so
+// the batch keeps the second run's result (its dose buffer is cleared in
+// between).
+static int tuned_cccs(fd2_context* ctx, size_t nb, int P, const fd2_cccs_kernel* k, cudaStream_t st,
+                      const std::function<int(int)>& run, float* dD, size_t n_dose) {
+    int bucket = 0;
+    while (((size_t)1 << (bucket + 1)) <= nb) bucket++;
+    const uint64_t key = (uint64_t)bucket | (uint64_t)P << 8 | (uint64_t)k->n_phi << 24 | (uint64_t)k->n_theta << 40;
+    auto it = ctx->cccs_schedule.find(key);
+    if (it != ctx->cccs_schedule.end()) return run(it->second);
+    cudaEvent_t ev[3];
+    for (auto& e : ev) FD2_CHECK_CUDA(cudaEventCreate(&e));
+    int rc = FD2_OK;
+    float ms[2] = {0.0f, 0.0f};
+    if (cudaEventRecord(ev[0], st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    if (!rc) rc = run(0);
+    if (!rc && cudaEventRecord(ev[1], st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    if (!rc && cudaMemsetAsync(dD, 0, n_dose * sizeof(float), st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    cudaEvent_t mid = nullptr;
+    if (!rc && cudaEventCreate(&mid) == cudaSuccess) cudaEventRecord(mid, st);
+    if (!rc) rc = run(1);
+    if (!rc && cudaEventRecord(ev[2], st) != cudaSuccess) rc = FD2_ERR_CUDA;
+    if (!rc && cudaEventSynchronize(ev[2]) != cudaSuccess) rc = FD2_ERR_CUDA;
+    if (!rc) {
+        cudaEventElapsedTime(&ms[0], ev[0], ev[1]);
+        cudaEventElapsedTime(&ms[1], mid ? mid : ev[1], ev[2]);
+        ctx->cccs_schedule[key] = ms[1] < ms[0] ? 1 : 0;
+        ctx->tuning_runs++;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+    if (mid) cudaEventDestroy(mid);
+    return rc;
 }
 
 // Candidate voxels of each beamlet (the capacity of its row): geometry only,
@@ -409,9 +448,15 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
             }
             {
                 StageTimer t(ctx, st, FD2_STAGE_CCCS);
-                int sched = params.cccs_schedule >= 0 ? params.cccs_schedule : cccs_auto_schedule(ctx, nb);
-                FD2_TRY(launch_cccs_host(ctx, nb, beams.data() + b0, d_beams + b0, (const float* const*)aT,
-                                         (const float* const*)aR, aD, kernel, sched, st));
+                auto run = [&](int sched) {
+                    return launch_cccs_host(ctx, nb, beams.data() + b0, d_beams + b0, (const float* const*)aT,
+                                            (const float* const*)aR, aD, kernel, sched, st);
+                };
+                if (params.cccs_schedule >= 0) {
+                    FD2_TRY(run(params.cccs_schedule));
+                } else {
+                    FD2_TRY(tuned_cccs(ctx, nb, P, kernel, st, run, dD, off[nb]));
+                }
                 t.stop();
             }
             StageTimer t(ctx, st, FD2_STAGE_COLUMNS);

@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/fd2.h"
@@ -70,6 +71,9 @@ struct fd2_context {
     uint64_t launches = 0;
     int timing = 0;
     double stage_ms[FD2_STAGE_COUNT] = {0};
+    // autotuned CCCS schedule (0 or 1) per batch shape, measured on first use
+    std::unordered_map<uint64_t, int> cccs_schedule;
+    uint64_t tuning_runs = 0;  // batches on which both schedules were timed
 };
 
 namespace fd2 {

@@ -148,6 +148,15 @@ int fd2_context_set_timing(fd2_context* ctx, int on);
 int fd2_context_stage_times(fd2_context* ctx, double* ms, int n);
 /* Number of kernels this library launched through the context so far. */
 uint64_t fd2_context_launch_count(const fd2_context* ctx);
+/*
+ * The context's tuned CCCS schedules (the construction's automatic choice,
+ * measured once per batch shape): up to cap (shape key, schedule) pairs and
+ * their number in *n; *runs = batches on which both schedules were timed.
+ * Key bits: 0-7 log2 of the batch's beamlets, 8-23 map pixels, 24-39 azimuths,
+ * 40- zenith bins.
+ */
+int fd2_context_tuned_schedules(const fd2_context* ctx, size_t cap, uint64_t* keys, int32_t* schedules, size_t* n,
+                                uint64_t* runs);
 
 /*
  * fastdose::density_h2d (FastDoseLib/src/density.cu:23-58).  Copies a host

@@ -88,6 +88,33 @@ def _dense(ro, col, val, n_rows, n_cols):
     return out
 
 
+def test_tuned_cccs_schedule(ctx):
+    """The automatic schedule times both schedules on the first batch of a
+    shape, then reuses the choice; every build gives the same matrix as either
+    fixed schedule, bit for bit."""
+    from fastdose_b200 import api as _api
+
+    c2 = _api.Context(0)  # a fresh context: no tuned shapes yet
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(c2, case)
+    fixed = [_api.DoseMatConstruction(c2, [case["beams"]], case["fluence"], dens, sp, kn, cccs_schedule=s)
+             for s in (0, 1)]
+    ref = [m.to_host() for m in fixed]
+    for a, b in zip(*ref):
+        np.testing.assert_array_equal(a, b)
+    assert c2.tuned_schedules() == ({}, 0)
+    for k in range(2):
+        m = _api.DoseMatConstruction(c2, [case["beams"]], case["fluence"], dens, sp, kn)
+        for a, b in zip(m.to_host(), ref[0]):
+            np.testing.assert_array_equal(a, b)
+        m.close()
+        sched, runs = c2.tuned_schedules()
+        assert runs == 1 and len(sched) == 1 and list(sched.values())[0] in (0, 1)
+    for h in fixed + [dens, sp, kn]:
+        h.close()
+    c2.close()
+
+
 def test_columns_match_oracle(ctx):
     case = small_case()
     beams, out, _, _ = _run_bev(ctx, case, list(range(16)))
