@@ -125,12 +125,15 @@ __global__ void add_vectors(const float* __restrict__ a, const float* __restrict
         out[i] = __fadd_rn(a[i], b[i]);  // d_elementWiseAdd
 }
 
-// y = (1 - theta) x + theta v
-__global__ void extrapolate(const float* __restrict__ x, const float* __restrict__ v, float theta,
+// y = (1 - theta) x + theta v when step[2] != 0, else y = x; theta = step[0]
+// (the trial's scalars come from device memory, so one captured graph serves
+// every trial)
+__global__ void extrapolate(const float* __restrict__ x, const float* __restrict__ v, const float* __restrict__ step,
                             float* __restrict__ y, int64_t n) {
-    const float a = 1.0f - theta;
+    const float theta = step[0], a = 1.0f - theta;
+    const bool ex = step[2] != 0.0f;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        y[i] = __fadd_rn(__fmul_rn(a, x[i]), __fmul_rn(theta, v[i]));
+        y[i] = ex ? __fadd_rn(__fmul_rn(a, x[i]), __fmul_rn(theta, v[i])) : x[i];
 }
 
 // v = (1/theta) x + (1 - 1/theta) xkm1 ; xkm1 = x
@@ -144,9 +147,10 @@ __global__ void momentum(const float* __restrict__ x, float iot, float* __restri
     }
 }
 
-// x = max(y - t g, 0)   (the polish projection)
-__global__ void project_step(const float* __restrict__ y, const float* __restrict__ g, float t, float* __restrict__ x,
-                             int64_t n) {
+// x = max(y - t g, 0)   (the polish projection), t = *t_dev
+__global__ void project_step(const float* __restrict__ y, const float* __restrict__ g, const float* __restrict__ t_dev,
+                             float* __restrict__ x, int64_t n) {
+    const float t = *t_dev;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         x[i] = fmaxf(__fadd_rn(y[i], __fmul_rn(-t, g[i])), 0.0f);
 }
@@ -166,11 +170,13 @@ __device__ __forceinline__ float t_hat(float nrm2, float tau) {
 
 // One block per group: in = max(y - t g, 0) (or y itself when g is null),
 // prox = tHat(||in||^2, tau) in, nrm = ||prox||, with FP64 norm sums.
-// tau = tau[r] when given, else w[r] * t.
+// tau = tau[r] when given, else w[r] * t; t = *t_dev when t_dev is given.
 __global__ void __launch_bounds__(kRedThreads) group_prox(const int64_t* __restrict__ go, const float* __restrict__ y,
                                                           const float* __restrict__ g, float t,
+                                                          const float* __restrict__ t_dev,
                                                           const float* __restrict__ w, const float* __restrict__ tau,
                                                           float* __restrict__ x, float* __restrict__ nrm) {
+    if (t_dev) t = *t_dev;
     typedef cub::BlockReduce<double, kRedThreads> R;
     __shared__ typename R::TempStorage tmp;
     __shared__ float s_th;
@@ -248,6 +254,15 @@ struct fd2_opt_problem {
     float *d_y = nullptr, *d_g = nullptr, *d_x = nullptr;
     double *d_part = nullptr, *d_red = nullptr;
     double* h_red = nullptr;  // pinned [S_COUNT]
+    // the trial's scalars (theta, t, extrapolated) in pinned host memory and
+    // on the device, and the trial captured as a CUDA graph
+    float* h_step = nullptr;  // pinned [4]
+    float* d_step = nullptr;  // [4]
+    bool use_graph = true;
+    cudaGraphExec_t trial_exec = nullptr;
+    const float *graph_xkm1 = nullptr, *graph_vkm1 = nullptr;
+    int64_t graph_groups = -1;
+    uint64_t graph_kernels = 0;
     // group buffers (BOO)
     int64_t groups_cap = 0;
     int64_t* d_go = nullptr;
@@ -301,8 +316,11 @@ int read_scalars(fd2_opt_problem* p, int64_t n_groups) {
     return FD2_OK;
 }
 
+void drop_graph(fd2_opt_problem* p);
+
 int ensure_groups(fd2_opt_problem* p, int64_t n_groups) {
     if (n_groups <= p->groups_cap) return FD2_OK;
+    drop_graph(p);  // its copies name the group buffers being replaced
     FD2_TRY(palloc(p, (void**)&p->d_go, (n_groups + 1) * sizeof(int64_t)));
     FD2_TRY(palloc(p, (void**)&p->d_w, n_groups * sizeof(float)));
     FD2_TRY(palloc(p, (void**)&p->d_nrm, n_groups * sizeof(float)));
@@ -315,25 +333,79 @@ int ensure_groups(fd2_opt_problem* p, int64_t n_groups) {
 
 // One line-search trial at step t: y from (theta, xkm1, vkm1); x = prox or
 // projection of y - t grad g(y); leaves gx, gy, <grad, x - y>, ||x - y||^2 in h_red.
-int trial(fd2_opt_problem* p, const fd2_opt_state_t* st, float theta, bool extrapolated, float t, int64_t n_groups) {
+// The work of one trial, enqueued on the context's stream without a host
+// wait: the scalars' upload, the products and reductions, the read-back of
+// the four scalars and the group norms into pinned memory.
+int trial_enqueue(fd2_opt_problem* p, const fd2_opt_state_t* st, int64_t n_groups) {
     cudaStream_t s = p->ctx->stream;
     const int64_t n = p->n;
-    if (extrapolated)
-        extrapolate<<<vec_blocks(n), 256, 0, s>>>(st->d_xkm1, st->d_vkm1, theta, p->d_y, n);
-    else
-        FD2_CHECK_CUDA(cudaMemcpyAsync(p->d_y, st->d_xkm1, n * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    FD2_CHECK_CUDA(cudaMemcpyAsync(p->d_step, p->h_step, 4 * sizeof(float), cudaMemcpyHostToDevice, s));
+    extrapolate<<<vec_blocks(n), 256, 0, s>>>(st->d_xkm1, st->d_vkm1, p->d_step, p->d_y, n);
     FD2_TRY(objective(p, p->d_y, p->d_g, S_GY));
     if (n_groups > 0)
-        group_prox<<<(unsigned)n_groups, kRedThreads, 0, s>>>(p->d_go, p->d_y, p->d_g, t, p->d_w, nullptr, p->d_x,
-                                                              p->d_nrm);
+        group_prox<<<(unsigned)n_groups, kRedThreads, 0, s>>>(p->d_go, p->d_y, p->d_g, 0.0f, p->d_step + 1, p->d_w,
+                                                              nullptr, p->d_x, p->d_nrm);
     else
-        project_step<<<vec_blocks(n), 256, 0, s>>>(p->d_y, p->d_g, t, p->d_x, n);
+        project_step<<<vec_blocks(n), 256, 0, s>>>(p->d_y, p->d_g, p->d_step + 1, p->d_x, n);
     FD2_TRY(objective(p, p->d_x, nullptr, S_GX));
     step_terms<<<kRedBlocks, kRedThreads, 0, s>>>(p->d_g, p->d_x, p->d_y, n, p->d_part);
     finish_sums<2><<<1, kRedThreads, 0, s>>>(p->d_part, kRedBlocks, p->d_red + S_DXY);
     FD2_CHECK_CUDA(cudaGetLastError());
-    p->ctx->launches += 4;
-    return read_scalars(p, n_groups);
+    p->ctx->launches += 5;
+    FD2_CHECK_CUDA(cudaMemcpyAsync(p->h_red, p->d_red, S_COUNT * sizeof(double), cudaMemcpyDeviceToHost, s));
+    if (n_groups > 0)
+        FD2_CHECK_CUDA(cudaMemcpyAsync(p->h_nrm, p->d_nrm, n_groups * sizeof(float), cudaMemcpyDeviceToHost, s));
+    return FD2_OK;
+}
+
+void drop_graph(fd2_opt_problem* p) {
+    if (p->trial_exec) cudaGraphExecDestroy(p->trial_exec);
+    p->trial_exec = nullptr;
+    p->graph_groups = -1;
+}
+
+// The trial's launches as one CUDA graph, captured for this state's vectors and
+// group count; replays read the scalars from p->h_step at execution.
+int capture_trial(fd2_opt_problem* p, const fd2_opt_state_t* st, int64_t n_groups) {
+    drop_graph(p);
+    cudaStream_t s = p->ctx->stream;
+    const uint64_t before = p->ctx->launches;
+    FD2_CHECK_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    const int rc = trial_enqueue(p, st, n_groups);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(s, &graph);
+    if (rc || e != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        if (!rc) FD2_CHECK_CUDA(e);
+        return rc;
+    }
+    const cudaError_t ei = cudaGraphInstantiate(&p->trial_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    FD2_CHECK_CUDA(ei);
+    p->graph_xkm1 = st->d_xkm1;
+    p->graph_vkm1 = st->d_vkm1;
+    p->graph_groups = n_groups;
+    p->graph_kernels = p->ctx->launches - before;
+    p->ctx->launches = before;
+    return FD2_OK;
+}
+
+int trial(fd2_opt_problem* p, const fd2_opt_state_t* st, float theta, bool extrapolated, float t, int64_t n_groups) {
+    cudaStream_t s = p->ctx->stream;
+    p->h_step[0] = theta;
+    p->h_step[1] = t;
+    p->h_step[2] = extrapolated ? 1.0f : 0.0f;
+    if (p->use_graph) {
+        if (!p->trial_exec || p->graph_xkm1 != st->d_xkm1 || p->graph_vkm1 != st->d_vkm1 ||
+            p->graph_groups != n_groups)
+            FD2_TRY(capture_trial(p, st, n_groups));
+        FD2_CHECK_CUDA(cudaGraphLaunch(p->trial_exec, s));
+        p->ctx->launches += p->graph_kernels;
+    } else {
+        FD2_TRY(trial_enqueue(p, st, n_groups));
+    }
+    FD2_CHECK_CUDA(cudaStreamSynchronize(s));
+    return FD2_OK;
 }
 
 // theta of the accelerated step (IMRTOptimize.cu:78-84): the positive root of
@@ -469,6 +541,8 @@ int fd2_opt_problem_create(fd2_context* ctx, const fd2_matrix* A, const fd2_matr
     if (!rc) rc = palloc(p, (void**)&p->d_part, (size_t)kRedBlocks * kTerms * sizeof(double));
     if (!rc) rc = palloc(p, (void**)&p->d_red, S_COUNT * sizeof(double));
     if (!rc && cudaMallocHost(&p->h_red, S_COUNT * sizeof(double)) != cudaSuccess) rc = FD2_ERR_OUT_OF_MEMORY;
+    if (!rc && cudaMallocHost(&p->h_step, 4 * sizeof(float)) != cudaSuccess) rc = FD2_ERR_OUT_OF_MEMORY;
+    if (!rc) rc = palloc(p, (void**)&p->d_step, 4 * sizeof(float));
     if (!rc && cudaMemsetAsync(p->d_red, 0, S_COUNT * sizeof(double), st) != cudaSuccess) rc = FD2_ERR_CUDA;
     if (!rc && cudaStreamSynchronize(st) != cudaSuccess) rc = FD2_ERR_CUDA;
     if (rc) {
@@ -481,10 +555,19 @@ int fd2_opt_problem_create(fd2_context* ctx, const fd2_matrix* A, const fd2_matr
 
 int fd2_opt_problem_destroy(fd2_opt_problem* p) {
     if (!p) return FD2_OK;
+    drop_graph(p);
     for (void* q : p->owned) cudaFree(q);
     if (p->h_red) cudaFreeHost(p->h_red);
+    if (p->h_step) cudaFreeHost(p->h_step);
     if (p->h_nrm) cudaFreeHost(p->h_nrm);
     delete p;
+    return FD2_OK;
+}
+
+int fd2_opt_problem_set_graph(fd2_opt_problem* p, int on) {
+    FD2_REQUIRE(p, FD2_ERR_INVALID_ARGUMENT, "opt_problem_set_graph: null problem");
+    p->use_graph = on != 0;
+    if (!p->use_graph) drop_graph(p);
     return FD2_OK;
 }
 
@@ -510,7 +593,7 @@ int fd2_prox_l2onehalf(fd2_context* ctx, int64_t n_groups, const int64_t* d_go, 
                 "prox_l2onehalf: null argument");
     if (n_groups <= 0) return FD2_OK;
     group_prox<<<(unsigned)n_groups, kRedThreads, 0, (cudaStream_t)stream>>>(d_go, d_g0, nullptr, 0.0f, nullptr,
-                                                                             d_tau, d_prox, d_nrm);
+                                                                             nullptr, d_tau, d_prox, d_nrm);
     FD2_CHECK_CUDA(cudaGetLastError());
     ctx->launches += 1;
     return FD2_OK;

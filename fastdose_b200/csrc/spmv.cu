@@ -526,8 +526,7 @@ cudaError_t allow_smem_x() {
 
 template <typename T, bool kPacked>
 int launch_stream_fmt(const fd2_matrix* m, const StreamArgs& a, const float* x, float* y, cudaStream_t st) {
-    if (m->x_in_smem) {
-        FD2_CHECK_CUDA((allow_smem_x<T, kPacked>()));
+    if (m->x_in_smem) {  // the shared-memory limit was raised when the matrix was finalized
         const unsigned blocks = (unsigned)(((int64_t)m->n_warps * 32 + kSmemThreads - 1) / kSmemThreads);
         spmv_stream_kernel<T, kPacked, true><<<blocks, kSmemThreads, (size_t)m->cols * sizeof(float), st>>>(a, x, y);
     } else {

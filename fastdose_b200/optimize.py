@@ -229,6 +229,10 @@ class Problem:
         _join_torch()
         return st, x, v, loss, nrm
 
+    def set_graph(self, on):
+        """Trials replayed from one captured CUDA graph (default) or launched one by one."""
+        _lib.check(self.ctx.lib.fd2_opt_problem_set_graph(self.h, int(on)), "opt_problem_set_graph")
+
     def boo(self, group_offsets, beam_weights, x0, step_size, iters, prune=(), want=0, change_trigger=100,
             show=100, state=None):
         """BOO_IMRT_L2OneHalf_gpu_QL; returns the solver state and outputs."""

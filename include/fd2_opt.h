@@ -144,6 +144,13 @@ int fd2_opt_problem_create(fd2_context* ctx, const fd2_matrix* A, const fd2_matr
                            const float* h_max_weights, const float* h_min_dose, const float* h_min_weights,
                            const float* h_oar_weights, float gamma, float eta, fd2_opt_problem** out);
 int fd2_opt_problem_destroy(fd2_opt_problem* p);
+/*
+ * Line-search trials as one CUDA graph (default on): the trial's kernels and
+ * copies are captured once per solver call (per state vectors and group
+ * count) and replayed with the trial's scalars read from pinned memory.  Off:
+ * the same launches one by one.  Results are identical either way.
+ */
+int fd2_opt_problem_set_graph(fd2_opt_problem* p, int on);
 
 /* eval_g::evaluate: *h_value = g(d_x) (synchronises the context's stream). */
 int fd2_eval_g(fd2_opt_problem* p, const float* d_x, double* h_value);

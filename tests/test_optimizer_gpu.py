@@ -241,6 +241,23 @@ def test_boo_matches_oracle(ctx):
     assert np.abs(x - ref["x"]).max() <= 1e-2 * max(np.abs(ref["x"]).max(), 1e-6)
 
 
+def test_trials_from_a_captured_graph_match_direct_launches(ctx):
+    """BOO and polish give the same bits whether each line-search trial is
+    replayed from the captured CUDA graph or launched kernel by kernel."""
+    A, D, w, groups, n_ptv, n_oar, n = _problem_case(seed=14)
+    x0 = np.full(n, 0.01, np.float32)
+    out = []
+    for graph in (True, False):
+        P = _gpu_problem(ctx, A, D, w, n_ptv, n_oar, n)
+        P.set_graph(graph)
+        bw = 0.1 * P.beam_weights_init(groups)
+        r = P.boo(groups, bw, x0, step_size=1e-3, iters=40, want=2, change_trigger=10)
+        q = P.polish(x0, step_size=1e-3, iters=30)
+        out.append((r["loss"], r["x"].cpu().numpy(), r["nrm"], r["trials"], q["loss"], q["x"].cpu().numpy()))
+    for a, b in zip(*out):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_polish_matches_oracle(ctx):
     A, D, w, groups, n_ptv, n_oar, n = _problem_case(seed=12)
     P = _gpu_problem(ctx, A, D, w, n_ptv, n_oar, n)
