@@ -715,6 +715,25 @@ def run_fd2(args, rank, world):
     cccs_ms = stages["cccs"]
     peak, peak_kind = _peaks()
     achieved = cccs_bytes / (cccs_ms * 1e-3) / 1e9 if cccs_ms > 0 else None
+    # The march's special-function roof: each ray step costs 3 MUFU operations
+    # (two exp2, one rsqrt) for each of the P rays; a base ray in normalised BEV
+    # units (pixels laterally, slices in depth) crosses L (1 + (|dx| + |dy|) / dz)
+    # voxel boundaries over the L slices of one (zenith, azimuth) pass.  Peak: 16
+    # MUFU results per clock per SM (the CUDA throughput table) at the sampled clock.
+    dirs = api.cone_directions(ctx, kern, np.concatenate(beamlets))  # [beamlet, theta, phi, 4]
+    ratio = (np.abs(dirs[..., 0]) + np.abs(dirs[..., 1])) / np.maximum(dirs[..., 2], 1e-6)
+    ray_steps = float(np.sum(L[:, None, None] * (1.0 + ratio)))
+    sfu_ops = ray_steps * P * 3.0
+    clk_now = clk.summary()
+    sm_mhz = clk_now.get("sm_mhz") or 1965.0
+    sfu_peak = 16.0 * (torch.cuda.get_device_properties(dev).multi_processor_count) * sm_mhz * 1e6
+    sfu_achieved = sfu_ops / (cccs_ms * 1e-3) if cccs_ms > 0 else None
+    # The whole pipeline against HBM under the compulsory-traffic convention:
+    # per beamlet Terma and density written and read, dose written and read
+    # (4 P L 6), the density footprint read once (taken as its nonzero count),
+    # the column's value and index written (4 + 4 per nonzero), and the offsets.
+    pipe_bytes = float(np.sum(4.0 * P * L * 6)) + float(info["nnz"]) * (4 + 4 + 4) + 8.0 * (n_bl + 1)
+    pipe_ms = ms / args.steps
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -731,8 +750,18 @@ def run_fd2(args, rank, world):
         "roofline": {"bound": "hbm", "kernel": "cccs_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak if achieved else None, "traffic": cccs_traffic,
                      "peak_source": peak_kind, "algorithmic_bytes_per_step": cccs_bytes},
+        "sfu_roofline": {"bound": "MUFU", "kernel": "cccs_kernel", "ops_per_step": sfu_ops, "ray_steps": ray_steps,
+                         "achieved_ops_per_s": sfu_achieved, "peak_ops_per_s": sfu_peak,
+                         "frac": sfu_achieved / sfu_peak if sfu_achieved else None,
+                         "basis": "3 MUFU per ray step; ray steps L (1 + (|dx|+|dy|)/dz) per cone pass from the "
+                                  "device's cone directions; peak 16/clk/SM at the sampled SM clock"},
+        "pipeline_roofline": {"bound": "hbm", "bytes_per_step": pipe_bytes, "ms_per_step": pipe_ms,
+                              "achieved": pipe_bytes / (pipe_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                              "frac": pipe_bytes / (pipe_ms * 1e-3) / 1e9 / peak,
+                              "basis": "per beamlet 4 P L 6 + 4 per footprint voxel (taken as its nonzeros) + "
+                                       "8 per nonzero (value, index) + 8 per row offset"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "clocks": clk.summary(),
+        "clocks": clk_now,
     }
     if not args.no_extras:
         sb = single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream)
