@@ -259,6 +259,10 @@ struct fd2_opt_problem {
     float* h_step = nullptr;  // pinned [4]
     float* d_step = nullptr;  // [4]
     bool use_graph = true;
+    // row-sharded problems: the caller's sum over ranks of a device FP64 buffer
+    fd2_reduce_fn reducer = nullptr;
+    void* reducer_user = nullptr;
+    double* d_rbuf = nullptr;  // [n + 3]
     cudaGraphExec_t trial_exec = nullptr;
     const float *graph_xkm1 = nullptr, *graph_vkm1 = nullptr;
     int64_t graph_groups = -1;
@@ -280,6 +284,40 @@ int palloc(fd2_opt_problem* p, void** ptr, size_t bytes) {
     return FD2_OK;
 }
 
+// Row-sharded problems: buf = [the three VOI-row terms, the partial A^T g1]
+// in FP64, summed over the ranks by the caller's reducer, and unpacked.  The
+// fluence-gradient terms and D^T g2 are the same on every rank and stay local.
+__global__ void pack_partials(const double* __restrict__ terms, const float* __restrict__ o1, int64_t n,
+                              double* __restrict__ buf) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n + 3; i += stride)
+        buf[i] = i < 3 ? terms[i] : (double)o1[i - 3];
+}
+__global__ void unpack_partials(const double* __restrict__ buf, int64_t n, double* __restrict__ terms,
+                                float* __restrict__ o1) {
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n + 3; i += stride) {
+        if (i < 3)
+            terms[i] = buf[i];
+        else
+            o1[i - 3] = (float)buf[i];
+    }
+}
+
+int reduce_partials(fd2_opt_problem* p, bool with_grad) {
+    cudaStream_t st = p->ctx->stream;
+    const int64_t n = with_grad ? p->n : 0;
+    pack_partials<<<vec_blocks(n + 3), 256, 0, st>>>(p->d_red + S_TERMS, p->d_o1, n, p->d_rbuf);
+    FD2_CHECK_CUDA(cudaGetLastError());
+    FD2_CHECK_CUDA(cudaStreamSynchronize(st));  // the reducer works on its own stream
+    const int rc = p->reducer(p->reducer_user, p->d_rbuf, n + 3, st);
+    FD2_REQUIRE(rc == 0, FD2_ERR_CUDA, "optimizer: the rank reduction failed (%d)", rc);
+    unpack_partials<<<vec_blocks(n + 3), 256, 0, st>>>(p->d_rbuf, n, p->d_red + S_TERMS, p->d_o1);
+    FD2_CHECK_CUDA(cudaGetLastError());
+    p->ctx->launches += 2;
+    return FD2_OK;
+}
+
 // objective of x into d_red[slot]; with grad: the gradient into grad
 int objective(fd2_opt_problem* p, const float* x, float* grad, int slot) {
     cudaStream_t st = p->ctx->stream;
@@ -290,9 +328,8 @@ int objective(fd2_opt_problem* p, const float* x, float* grad, int slot) {
                                                         p->eta, grad ? p->d_g1 : nullptr, grad ? p->d_g2 : nullptr,
                                                         p->d_part);
     finish_sums<kTerms><<<1, kRedThreads, 0, st>>>(p->d_part, kRedBlocks, p->d_red + S_TERMS);
-    objective_value<<<1, 32, 0, st>>>(p->d_red + S_TERMS, p->gamma, p->eta, p->d_red, slot);
     FD2_CHECK_CUDA(cudaGetLastError());
-    p->ctx->launches += 3;
+    p->ctx->launches += 2;
     if (grad) {
         if (p->m) {
             FD2_TRY(matrix_spmv(p->DT, p->d_g2, p->d_o2, st));
@@ -300,10 +337,15 @@ int objective(fd2_opt_problem* p, const float* x, float* grad, int slot) {
             FD2_CHECK_CUDA(cudaMemsetAsync(p->d_o2, 0, p->n * sizeof(float), st));
         }
         FD2_TRY(matrix_spmv(p->AT, p->d_g1, p->d_o1, st));
+    }
+    if (p->reducer) FD2_TRY(reduce_partials(p, grad != nullptr));
+    objective_value<<<1, 32, 0, st>>>(p->d_red + S_TERMS, p->gamma, p->eta, p->d_red, slot);
+    p->ctx->launches += 1;
+    if (grad) {
         add_vectors<<<vec_blocks(p->n), 256, 0, st>>>(p->d_o1, p->d_o2, grad, p->n);
-        FD2_CHECK_CUDA(cudaGetLastError());
         p->ctx->launches += 1;
     }
+    FD2_CHECK_CUDA(cudaGetLastError());
     return FD2_OK;
 }
 
@@ -566,8 +608,20 @@ int fd2_opt_problem_destroy(fd2_opt_problem* p) {
 
 int fd2_opt_problem_set_graph(fd2_opt_problem* p, int on) {
     FD2_REQUIRE(p, FD2_ERR_INVALID_ARGUMENT, "opt_problem_set_graph: null problem");
-    p->use_graph = on != 0;
+    p->use_graph = on != 0 && !p->reducer;
     if (!p->use_graph) drop_graph(p);
+    return FD2_OK;
+}
+
+int fd2_opt_problem_set_reducer(fd2_opt_problem* p, fd2_reduce_fn fn, void* user) {
+    FD2_REQUIRE(p, FD2_ERR_INVALID_ARGUMENT, "opt_problem_set_reducer: null problem");
+    p->reducer = fn;
+    p->reducer_user = user;
+    if (fn) {
+        p->use_graph = false;  // the reduction is a host call between kernels
+        drop_graph(p);
+        if (!p->d_rbuf) FD2_TRY(palloc(p, (void**)&p->d_rbuf, (p->n + 3) * sizeof(double)));
+    }
     return FD2_OK;
 }
 
@@ -605,8 +659,8 @@ int fd2_beam_weights_init(fd2_opt_problem* p, int64_t n_groups, const int64_t* h
                 "beam_weights_init: groups must cover the %lld beamlets", (long long)p->n);
     const fd2_matrix* at = p->AT;
     cudaStream_t st = p->ctx->stream;
-    double* d_s = nullptr;
-    FD2_CHECK_CUDA(cudaMalloc(&d_s, std::max<int64_t>(at->rows, 1) * sizeof(double)));
+    double* d_s = nullptr;  // [rows] PTV sums, then this problem's PTV row count (summed over ranks)
+    FD2_CHECK_CUDA(cudaMalloc(&d_s, (at->rows + 1) * sizeof(double)));
     const float* rs = at->scale_axis == FD2_SCALE_ROWS ? at->d_scale : nullptr;
     const unsigned blocks = (unsigned)((at->rows * 32 + 255) / 256);
     if (at->rows) {
@@ -624,20 +678,33 @@ int fd2_beam_weights_init(fd2_opt_problem* p, int64_t n_groups, const int64_t* h
                                                               at->rows, p->n_ptv, d_s);
         }
     }
-    std::vector<double> s(at->rows);
+    std::vector<double> s(at->rows + 1);
+    s[at->rows] = (double)p->n_ptv;
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess && at->rows)
-        e = cudaMemcpyAsync(s.data(), d_s, at->rows * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_s + at->rows, &s[at->rows], sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && p->reducer) {  // the PTV rows are spread over the ranks
+        e = cudaStreamSynchronize(st);
+        if (e == cudaSuccess && p->reducer(p->reducer_user, d_s, at->rows + 1, st) != 0) {
+            cudaFree(d_s);
+            set_error("beam_weights_init: the rank reduction failed");
+            return FD2_ERR_CUDA;
+        }
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s.data(), d_s, (at->rows + 1) * sizeof(double), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     cudaFree(d_s);
     FD2_CHECK_CUDA(e);
+    const double n_ptv = s[at->rows];  // all ranks' PTV rows
+    FD2_REQUIRE(n_ptv > 0, FD2_ERR_INVALID_ARGUMENT, "beam_weights_init: no PTV rows");
     // w_b = sqrt(sum_PTV A_b 1 / (n_ptv nbl_b)), normalised to the max, floored at 0.1
     float mx = 0.0f;
     for (int64_t b = 0; b < n_groups; b++) {
         double acc = 0;
         for (int64_t j = h_go[b]; j < h_go[b + 1]; j++) acc += s[j];
         const int64_t nb = h_go[b + 1] - h_go[b];
-        h_w[b] = std::sqrt((float)acc / (float)(p->n_ptv * nb));
+        h_w[b] = std::sqrt((float)acc / (float)((int64_t)n_ptv * nb));
         mx = std::max(mx, h_w[b]);
     }
     for (int64_t b = 0; b < n_groups; b++) {

@@ -229,6 +229,35 @@ class Problem:
         _join_torch()
         return st, x, v, loss, nrm
 
+    _REDUCE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p)
+
+    def set_reducer(self, fn):
+        """Row-sharded problem: fn(t) must replace the CUDA float64 tensor t by
+        its sum over the ranks (e.g. torch.distributed.all_reduce) before it
+        returns.  None restores the single-GPU problem."""
+        if fn is None:
+            self._reducer = None
+            _lib.check(self.ctx.lib.fd2_opt_problem_set_reducer(self.h, None, None), "opt_problem_set_reducer")
+            return
+        torch = _torch()
+
+        class _View:
+            def __init__(self, ptr, n):
+                self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False),
+                                                 "version": 3, "strides": None}
+
+        def cb(_user, ptr, n, _stream):
+            try:
+                fn(torch.as_tensor(_View(ptr, int(n)), device="cuda"))
+                torch.cuda.current_stream().synchronize()
+                return 0
+            except Exception:  # reported to the solver as a failed reduction
+                return 1
+
+        self._reducer = Problem._REDUCE(cb)  # kept alive with the problem
+        _lib.check(self.ctx.lib.fd2_opt_problem_set_reducer(self.h, C.cast(self._reducer, C.c_void_p), None),
+                   "opt_problem_set_reducer")
+
     def set_graph(self, on):
         """Trials replayed from one captured CUDA graph (default) or launched one by one."""
         _lib.check(self.ctx.lib.fd2_opt_problem_set_graph(self.h, int(on)), "opt_problem_set_graph")

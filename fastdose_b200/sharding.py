@@ -20,8 +20,11 @@ path:
 
 The optimizer shards the other way, by rows of A (voxels): `row_blocks` cuts
 the rows into contiguous blocks; A x is then local and the beamlet-space
-gradient is the sum of the blocks' partial A^T g, one all-reduce per
-evaluation (`allreduce_partials`).
+gradient is the sum of the blocks' partial A^T g.  The solver makes one
+all-reduce per objective evaluation, of the VOI-row objective terms and that
+partial gradient in one FP64 buffer, through the reducer the problem is given
+(`rank_reducer`, `optimize.Problem.set_reducer`); `allreduce_partials` is the
+same exchange for host-side code.
 """
 from __future__ import annotations
 
@@ -130,6 +133,18 @@ def row_blocks(n_rows: int, world: int) -> list[tuple[int, int]]:
         out.append((lo, hi))
         lo = hi
     return out
+
+
+def rank_reducer(group=None):
+    """The reducer a row-sharded optimizer problem takes
+    (optimize.Problem.set_reducer): the sum of a float64 tensor over the
+    group's ranks, in place (NCCL between GPU ranks)."""
+    import torch.distributed as dist
+
+    def fn(t):
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+
+    return fn
 
 
 def allreduce_partials(grad, terms, group=None):

@@ -152,6 +152,20 @@ int fd2_opt_problem_destroy(fd2_opt_problem* p);
  */
 int fd2_opt_problem_set_graph(fd2_opt_problem* p, int on);
 
+/*
+ * Row-sharded problems (one process per GPU, each holding a contiguous block
+ * of A's VOI rows, PTV rows first, with x, D and the weights of its rows): fn
+ * must replace d_buf[0..n) by its sum over the ranks before returning (e.g. an
+ * all-reduce over NCCL), on or after the given stream's work -- the solver has
+ * synchronised that stream before the call.  The solver calls it once per
+ * objective evaluation with the three VOI-row objective terms and, for a
+ * gradient, the partial A^T g (FP64), and once in fd2_beam_weights_init; every
+ * rank then takes the same steps.  A reducer turns graph capture off.  NULL
+ * restores the single-GPU problem.
+ */
+typedef int (*fd2_reduce_fn)(void* user, double* d_buf, int64_t n, void* stream);
+int fd2_opt_problem_set_reducer(fd2_opt_problem* p, fd2_reduce_fn fn, void* user);
+
 /* eval_g::evaluate: *h_value = g(d_x) (synchronises the context's stream). */
 int fd2_eval_g(fd2_opt_problem* p, const float* d_x, double* h_value);
 /* eval_grad::evaluate: d_grad[n] = grad g(d_x), *h_value = g(d_x). */

@@ -127,9 +127,14 @@ def _rank_main(rank, world, port, q):
         g = torch.from_numpy(A[lo:hi].T @ (w[lo:hi] * r)).to(torch.float32)
         terms = torch.tensor([0.5 * float(np.sum(w[lo:hi] * r * r)), float(hi - lo)], dtype=torch.float64)
         sharding.allreduce_partials(g, terms)
+        # the solver's reducer: an FP64 buffer summed over the ranks in place
+        buf = torch.full((5,), float(rank + 1), dtype=torch.float64)
+        sharding.rank_reducer()(buf)
+        ok_terms_r = bool(torch.all(buf == 3.0))
         rf = A @ x - d
         ok_grad = np.allclose(g.numpy(), (A.T @ (w * rf)).astype(np.float32), rtol=1e-6, atol=1e-5)
-        ok_terms = abs(terms[0].item() - 0.5 * float(np.sum(w * rf * rf))) < 1e-9 and terms[1].item() == n_rows
+        ok_terms = (abs(terms[0].item() - 0.5 * float(np.sum(w * rf * rf))) < 1e-9 and terms[1].item() == n_rows
+                    and ok_terms_r)
         if rank == 0:
             q.put(("merged", merged, parts))
         q.put(("opt", rank, ok_grad, ok_terms))
@@ -187,3 +192,95 @@ def test_sharded_construction_merges_to_the_whole_plan(ctx):
         merged = sharding.merge_ensembles(locals_, parts, [len(b) for b in beams])
         for a, b in zip(merged, whole):
             np.testing.assert_array_equal(a, b)
+
+
+@pytest.mark.gpu
+def test_row_sharded_optimizer_matches_the_whole_problem(ctx):
+    """The optimizer with A's VOI rows split between two ranks -- here two host
+    threads, each with its own context on the one GPU, exchanging partial sums
+    through host memory (no kernel waits on another) -- takes the same steps as
+    the whole problem: the same iterations and trials, costs within 1e-5 and the
+    same fluence within 1e-4 of its max (the partial sums are added in a
+    different order)."""
+    import threading
+
+    from fastdose_b200 import api, optimize
+
+    rng = np.random.default_rng(21)
+    n_beams, fd, per_beam, n_ptv, n_oar = 6, 8, 40, 500, 1500
+    n, nv = n_beams * per_beam, n_ptv + n_oar
+    dense = rng.random((nv, n)) * (rng.random((nv, n)) < 0.05)
+    import scipy.sparse as sp
+
+    A = sp.csr_matrix(dense.astype(np.float32))
+    masks = []
+    for _ in range(n_beams):
+        m = np.zeros(fd * fd, np.uint8)
+        m[rng.choice(fd * fd, per_beam, replace=False)] = 1
+        masks.append(m)
+    D = optimize.block_diag([optimize.fluence_grad(fd, m) for m in masks])
+    w = dict(max_dose=np.concatenate([np.full(n_ptv, 1.05), rng.uniform(0.3, 0.7, n_oar)]).astype(np.float32),
+             max_weights=np.concatenate([np.ones(n_ptv), rng.uniform(0.1, 1.0, n_oar)]).astype(np.float32),
+             min_dose=np.ones(n_ptv, np.float32), min_weights=np.ones(n_ptv, np.float32),
+             oar_weights=rng.uniform(0.0, 0.1, n_oar).astype(np.float32))
+    groups = np.arange(0, n + 1, per_beam, dtype=np.int64)
+    x0 = np.full(n, 0.01, np.float32)
+
+    def problem(c, lo, hi):
+        Ab = A[lo:hi]
+        Am = optimize.Matrix.from_csr(c, Ab.indptr.astype(np.int64), Ab.indices.astype(np.int64), Ab.data, n)
+        Dm = optimize.Matrix.from_csr(c, *D[:3], n)
+        p_lo, p_hi = min(lo, n_ptv), min(hi, n_ptv)
+        P = optimize.Problem(c, Am, Am.transpose(), Dm, Dm.transpose(), p_hi - p_lo, (hi - lo) - (p_hi - p_lo),
+                             w["max_dose"][lo:hi], w["max_weights"][lo:hi], w["min_dose"][p_lo:p_hi],
+                             w["min_weights"][p_lo:p_hi],
+                             w["oar_weights"][max(lo, n_ptv) - n_ptv:max(hi, n_ptv) - n_ptv], 1.0, 0.1)
+        return P, (Am, Dm)
+
+    def solve(P):
+        bw = 0.1 * P.beam_weights_init(groups)
+        r = P.boo(groups, bw, x0, step_size=1e-3, iters=40, want=2, change_trigger=10)
+        return dict(bw=bw, k=r["k"], trials=r["trials"], loss=r["loss"][:r["k"]], x=r["x"].cpu().numpy())
+
+    whole, _keep = problem(ctx, 0, nv)
+    ref = solve(whole)
+
+    blocks = sharding.row_blocks(nv, 2)
+    bar = threading.Barrier(2)
+    slots = [None, None]
+    out, errs = [None, None], []
+
+    def reducer(rank):
+        def fn(t):
+            slots[rank] = t.cpu().numpy()
+            bar.wait(timeout=60)
+            total = slots[0] + slots[1]  # the same order on both ranks
+            bar.wait(timeout=60)
+            t.copy_(torch.from_numpy(total).to(t.device))
+        return fn
+
+    def rank_main(rank):
+        try:
+            c = api.Context(0)
+            P, keep = problem(c, *blocks[rank])
+            P.set_reducer(reducer(rank))
+            out[rank] = solve(P)
+            P.close()
+            del keep
+        except Exception as e:  # surfaced below
+            errs.append(e)
+            bar.abort()
+
+    th = [threading.Thread(target=rank_main, args=(r,)) for r in range(2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(300)
+    assert not errs, errs
+    for r in range(2):
+        got = out[r]
+        np.testing.assert_allclose(got["bw"], ref["bw"], rtol=1e-6)
+        assert got["k"] == ref["k"] and got["trials"] == ref["trials"]
+        np.testing.assert_allclose(got["loss"], ref["loss"], rtol=1e-5)
+        assert np.abs(got["x"] - ref["x"]).max() <= 1e-4 * np.abs(ref["x"]).max()
+    np.testing.assert_array_equal(out[0]["x"], out[1]["x"])  # every rank takes the same steps
