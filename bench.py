@@ -159,7 +159,7 @@ def run_reference(args, rank):
     if flags is None:
         beams0 = np.array([api.calc_range(_bundle_beam(b), ph.volume) for b in bundles])
         flags = oracle.beamlet_flags(beams0, ph.masks["PTV"], ph.volume, tex_mode=1)
-    beamlets = [api.bundle_beamlets(b, f, ph.volume) for b, f in zip(bundles, flags)]
+    beamlets = api.bundles_beamlets(bundles, flags, ph.volume)
     fluence = api.beamlet_fluence(bundles[0])
     threads = os.cpu_count() or 1
     steps = []
@@ -398,8 +398,8 @@ def c4_leg(ctx, n_per_iso=300, opt_iters=20):
         beams, flags, fds = [], [], []
         for fd in np.unique(iso["fluence_dims"]):  # one flag pass per fluence dimension
             idx = np.flatnonzero(iso["fluence_dims"] == fd)
-            for j, f in zip(idx, api.beamletFlagInit(ctx, bundles[idx], iso["mask"], ph.volume)):
-                b = api.bundle_beamlets(bundles[j], f, ph.volume)
+            fl = api.beamletFlagInit(ctx, bundles[idx], iso["mask"], ph.volume)
+            for j, f, b in zip(idx, fl, api.bundles_beamlets(bundles[idx], fl, ph.volume)):
                 if len(b):
                     beams.append(b)
                     flags.append(np.asarray(f).reshape(-1))
@@ -488,8 +488,7 @@ def served_requests(ctx, n_requests, seed=11):
         bundles = np.array([make_bundle(iso, angles[j], sad=100.0, fluence_dim=16, beamlet_size=0.5,
                                         sub_fluence_dim=16, sub_fluence_on=4, long_spacing=0.25) for j in sel])
         flags = api.beamletFlagInit(ctx, bundles, ph.masks["PTV"], ph.volume)
-        beams = [api.bundle_beamlets(b, f, ph.volume) for b, f in zip(bundles, flags)]
-        beams = [b for b in beams if len(b)]
+        beams = [b for b in api.bundles_beamlets(bundles, flags, ph.volume) if len(b)]
         if beams:
             reqs.append(dict(phantom=ph, beams=beams, fluence=api.beamlet_fluence(bundles[0])))
     return reqs
@@ -607,7 +606,7 @@ def run_fd2(args, rank, world):
     cfg, bundles = plan_inputs(args.beams * world)
     ph = cfg["phantom"]
     flags = api.beamletFlagInit(ctx, bundles, ph.masks["PTV"], ph.volume)
-    all_beamlets = [api.bundle_beamlets(b, f, ph.volume) for b, f in zip(bundles, flags)]
+    all_beamlets = api.bundles_beamlets(bundles, flags, ph.volume)
     parts = sharding.partition_beams(sharding.beam_costs(all_beamlets), world)
     beamlets = [all_beamlets[i] for i in parts[rank]]
     n_bl_total = int(sum(len(b) for b in all_beamlets))

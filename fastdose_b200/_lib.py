@@ -78,6 +78,7 @@ _PROTOS = {
     "fd2_context_tuned_schedules": (_i, [_vp, _sz, _vp, _vp, _vp, _vp]),
     "fd2_opt_problem_set_graph": (_i, [_vp, _i]),
     "fd2_opt_problem_set_reducer": (_i, [_vp, _vp, _vp]),
+    "fd2_bundles_beamlets": (_i, [_sz, _vp, _vp, _vp, _i, _sz, _vp, _vp]),
     "fd2_beam_orientation_optimization": (_i, [_vp, _vp, _vp, _i64, _vp, _vp, _i64, _i64, _vp, _vp, _vp, _vp, _vp,
                                                 _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     # served dose calculation (fd2_service.h)

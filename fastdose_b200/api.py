@@ -67,6 +67,25 @@ def bundle_beamlets(bundle, flags, volume):
     return np.array(out, BEAM_DTYPE)
 
 
+def bundles_beamlets(bundles, flags, volume, threads=0):
+    """bundle_beamlets for many bundles in one native call over host threads:
+    a list of BEAM_DTYPE arrays, one per bundle (the same beams, bit for bit)."""
+    bb = np.ascontiguousarray(bundles, BUNDLE_DTYPE).reshape(-1)
+    fl = np.ascontiguousarray(np.concatenate([np.asarray(f, np.uint8).reshape(-1) for f in flags])
+                              if len(flags) else np.zeros(0, np.uint8))
+    total = int(np.count_nonzero(fl))
+    out = np.zeros(max(total, 1), BEAM_DTYPE)
+    counts = np.zeros(max(bb.size, 1), np.uint32)
+    v = np.array(volume, VOLUME_DTYPE)
+    _lib.check(_lib.get().fd2_bundles_beamlets(bb.size, _p(bb), _p(fl), _p(v), int(threads), out.size, _p(out),
+                                               _p(counts)), "bundles_beamlets")
+    res, o = [], 0
+    for c in counts[:bb.size]:
+        res.append(out[o:o + int(c)].copy())
+        o += int(c)
+    return res
+
+
 # ------------------------------------------------------------------ handles
 class Context:
     def __init__(self, device=0):

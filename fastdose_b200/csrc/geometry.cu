@@ -9,6 +9,9 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
 
 #include "fd2_internal.cuh"
 
@@ -235,6 +238,55 @@ int fd2_beam_calc_range(fd2_beam_t* beam, const fd2_volume_t* volume) {
 
 int fd2_beamlet_init(const fd2_bundle_t* bundle, int ix, int iy, const fd2_volume_t* volume, fd2_beam_t* out) {
     return fd2::beamlet_init(bundle, ix, iy, volume, out);
+}
+
+int fd2_bundles_beamlets(size_t n_bundles, const fd2_bundle_t* bundles, const uint8_t* flags,
+                         const fd2_volume_t* volume, int n_threads, size_t cap, fd2_beam_t* out, uint32_t* counts) {
+    FD2_REQUIRE((n_bundles == 0 || (bundles && flags && counts)) && volume && (cap == 0 || out),
+                FD2_ERR_INVALID_ARGUMENT, "bundles_beamlets: null argument");
+    // flagged pixels of each bundle, their flag offsets and output offsets
+    std::vector<size_t> foff(n_bundles + 1, 0), boff(n_bundles + 1, 0);
+    for (size_t b = 0; b < n_bundles; b++) {
+        const int fx = bundles[b].fluence_dim[0], fy = bundles[b].fluence_dim[1];
+        FD2_REQUIRE(fx > 0 && fy > 0, FD2_ERR_INVALID_ARGUMENT, "bundles_beamlets: bundle %zu has no fluence map", b);
+        foff[b + 1] = foff[b] + (size_t)fx * fy;
+        size_t c = 0;
+        for (size_t k = foff[b]; k < foff[b + 1]; k++) c += flags[k] != 0;
+        counts[b] = (uint32_t)c;
+        boff[b + 1] = boff[b] + c;
+    }
+    FD2_REQUIRE(boff[n_bundles] <= cap, FD2_ERR_CAPACITY, "bundles_beamlets: %zu beamlets, room for %zu",
+                boff[n_bundles], cap);
+    int threads = n_threads > 0 ? n_threads : (int)std::max(1u, std::thread::hardware_concurrency());
+    threads = (int)std::min<size_t>((size_t)threads, std::max<size_t>(n_bundles, 1));
+    std::mutex mu;
+    int first_rc = FD2_OK;
+    std::string first_msg;
+    auto work = [&](int t) {
+        for (size_t b = (size_t)t; b < n_bundles; b += (size_t)threads) {
+            const int fx = bundles[b].fluence_dim[0], fy = bundles[b].fluence_dim[1];
+            size_t o = boff[b];
+            for (int iy = 0; iy < fy; iy++)
+                for (int ix = 0; ix < fx; ix++) {
+                    if (!flags[foff[b] + (size_t)iy * fx + ix]) continue;
+                    const int rc = fd2::beamlet_init(&bundles[b], ix, iy, volume, &out[o++]);
+                    if (rc) {
+                        std::lock_guard<std::mutex> lock(mu);
+                        if (!first_rc) {
+                            first_rc = rc;
+                            first_msg = fd2_last_error();
+                        }
+                        return;
+                    }
+                }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < threads; t++) pool.emplace_back(work, t);
+    work(0);
+    for (auto& th : pool) th.join();
+    if (first_rc) fd2::set_error("%s", first_msg.c_str());
+    return first_rc;
 }
 
 int fd2_beamlet_fluence(const fd2_bundle_t* bb, float* out, size_t n) {

@@ -113,6 +113,18 @@ typedef struct fd2_bundle {
 int fd2_beamlet_init(const fd2_bundle_t* bundle, int ix, int iy,
                      const fd2_volume_t* volume, fd2_beam_t* out);
 
+/*
+ * BeamBundle::beamletsInit (IMRTBeamBundle.cu:319) for many bundles at once:
+ * fd2_beamlet_init for every flagged pixel of every bundle (raster order, y
+ * outer, x inner), spread over n_threads host threads (<= 0: one per core).
+ * h_flags holds each bundle's fy x fx flags, bundle after bundle (bundles may
+ * differ in fluence dimension).  out: room for cap beams, filled bundle after
+ * bundle; counts[b] = beamlets of bundle b.  Host only; the same beams, bit for
+ * bit, as one fd2_beamlet_init call per pixel.
+ */
+int fd2_bundles_beamlets(size_t n_bundles, const fd2_bundle_t* bundles, const uint8_t* h_flags,
+                         const fd2_volume_t* volume, int n_threads, size_t cap, fd2_beam_t* out, uint32_t* counts);
+
 /* Writes the sub-beam fluence map (float[fy][fx]) of a bundle into `out`. */
 int fd2_beamlet_fluence(const fd2_bundle_t* bundle, float* out, size_t n);
 

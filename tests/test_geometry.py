@@ -140,3 +140,33 @@ def test_sub_beam_fluence_is_centred_square():
     assert f.sum() == 16
     assert f[6:10, 6:10].all()
     np.testing.assert_array_equal(f.ravel(), oracle.beamlet_fluence(bund))
+
+
+def test_bundles_beamlets_equals_one_call_per_pixel():
+    """The batched, multi-threaded beamlet initialisation gives the same bytes
+    as one beamlet_init call per flagged pixel, for bundles of different
+    fluence dimensions, including empty flag maps."""
+    import numpy as np
+
+    from fastdose_b200 import api, phantoms
+    from fastdose_b200.types import make_bundle
+
+    cfg = phantoms.config2(12)
+    ph = cfg["phantom"]
+    rng = np.random.default_rng(3)
+    bundles, flags = [], []
+    for k, a in enumerate(cfg["angles"]):
+        fd = (8, 16, 11)[k % 3]
+        bundles.append(make_bundle(cfg["isocenter"], a, sad=100.0, fluence_dim=fd, beamlet_size=0.5,
+                                   sub_fluence_dim=16, sub_fluence_on=4, long_spacing=0.25))
+        f = (rng.random(fd * fd) < 0.4).astype(np.uint8)
+        if k == 5:
+            f[:] = 0
+        flags.append(f)
+    bundles = np.array(bundles)
+    ref = [api.bundle_beamlets(b, f, ph.volume) for b, f in zip(bundles, flags)]
+    for threads in (1, 4, 0):
+        got = api.bundles_beamlets(bundles, flags, ph.volume, threads=threads)
+        assert len(got) == len(ref)
+        for a, b in zip(ref, got):
+            assert a.tobytes() == b.tobytes()
