@@ -41,8 +41,10 @@ namespace fd2 {
 namespace {
 
 constexpr int kStepCap = 1 << 20;  // per-slice step cap (the watchdog bound)
-// The 16x16 march is compiled for at most 8 azimuth warps (register budget
-// for 4 such blocks of 256 threads, i.e. 5 blocks of 192 threads, per SM).
+// The 16x16 march is compiled for at most 8 azimuth warps and 5 such blocks
+// of 256 threads per SM (48 registers a thread), i.e. 7 blocks of 192 threads:
+// more resident azimuth warps hide the march's dependency chains and the
+// per-slice barrier (measured faster than 64 registers at 5 blocks of 192).
 constexpr int kFx16Threads = 256;
 
 struct RayGeom {  // per-beamlet scalars the march needs
@@ -137,13 +139,16 @@ __device__ __forceinline__ float seg_length(float l2) {
 
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
 // the current slice) followed by float2 dp[n_phi][P] (per-azimuth dose and path
-// sums).  RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
+// sums); for kFx16 instead float4 wb[n_phi][P] (each azimuth's copy of the
+// slice beside its sums) followed by float2 ytab[n_phi][16] (row tables).
+// RPL = rays per lane (P <= 32 * RPL); kFx16: the map is 16 x 16.
 // kCols: every map of the batch is F x F with F <= 32 -- each lane owns one
 // column (lane % F) and the rows lane / F + k j (k = 32 / F lanes per column),
 // so the x half of the voxel work is done once per lane and the y half once per
-// row and shared by shuffles, as for 16 x 16 maps; RPL >= ceil(F / k).
+// row and shared by shuffles (16 x 16 maps share it through the row table);
+// RPL >= ceil(F / k).
 template <int RPL, bool kFx16, bool kCols = false>
-__global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || (kCols && RPL <= 8) ? 4 : (kCols ? 3 : 1))
+__global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 5 : ((kCols && RPL <= 8) ? 4 : (kCols ? 3 : 1)))
     cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
@@ -181,10 +186,15 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || 
     float2* dp = smem + g.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float2* mydp = dp + (size_t)warp * g.P;
+    // kFx16: every azimuth warp keeps its own copy of the slice beside its sums,
+    // wb[warp][v] = {Terma, density, dose, path sum}, so a ray step reads all
+    // four with one 16-byte load; behind them, each warp's 16-entry row table.
+    float4* wb = reinterpret_cast<float4*>(smem);
+    float4* mywb = wb + (size_t)warp * g.P;
+    float2* ytab = reinterpret_cast<float2*>(wb + (size_t)n_phi * g.P) + 16 * warp;
     const float* __restrict__ T = terma[bi];
     const float* __restrict__ R = dens[bi];
     float* __restrict__ D = dose[bi];
-    const bool last_phi = warp == n_phi - 1;
 
     // per-ray constant pixel coordinates
     float fix[RPL], fiy[RPL];
@@ -229,13 +239,23 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || 
         __syncthreads();  // the previous pass has finished; s_next is visible
         int s = *s_next;
         while (s < g.L) {
-            if (s == pf_s) {
-                if (threadIdx.x < g.P) tr[threadIdx.x] = pf;
+            if constexpr (kFx16) {
+                // each pixel's pair goes to every azimuth's copy, sums cleared
+                for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
+                    const float2 t = s == pf_s ? pf
+                                               : make_float2(__ldg(T + (size_t)s * pitch + v),
+                                                             __ldg(R + (size_t)s * pitch + v));
+                    for (int w = 0; w < n_phi; w++) wb[(size_t)w * g.P + v] = make_float4(t.x, t.y, 0.0f, 0.0f);
+                }
             } else {
-                for (int v = threadIdx.x; v < g.P; v += blockDim.x)
-                    tr[v] = make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
+                if (s == pf_s) {
+                    if (threadIdx.x < g.P) tr[threadIdx.x] = pf;
+                } else {
+                    for (int v = threadIdx.x; v < g.P; v += blockDim.x)
+                        tr[v] = make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
+                }
+                for (int v = lane; v < g.P; v += 32) mydp[v] = make_float2(0.0f, 0.0f);
             }
-            for (int v = lane; v < g.P; v += 32) mydp[v] = make_float2(0.0f, 0.0f);
             __syncthreads();
             // Prefetch the slice most likely to come next (s + 1, or slice 0 of
             // the next zenith bin) into registers; its loads are in flight during
@@ -261,35 +281,42 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || 
                     const float lx = (float)(lane & 15);
                     const float btx = __fadd_rn(c.x, lx), ntx = __fadd_rn(np.x, lx);
                     const int cx = mid_index16(btx, ntx);
-                    const bool wrapx = crosses16(btx, ntx);
+                    const int wx = crosses16(btx, ntx) ? 256 : 0;
                     const float dxp = (ntx - 8.0f) * g.bsx * fe - (btx - 8.0f) * g.bsx * fs;
                     const float dxz2 = dxp * dxp + dzp * dzp;
                     // The y half depends only on the ray's row offset (16 values per
-                    // step): lane l computes it for row (l & 15), and each ray takes
-                    // its row's result by shuffle -- the same operations on the same
-                    // inputs as a per-ray evaluation, done once instead of 16 times.
-                    const float bty = __fadd_rn(c.y, lx), nty = __fadd_rn(np.y, lx);
-                    const int ycode = mid_index16(bty, nty) | (crosses16(bty, nty) ? 16 : 0);
-                    const float dyq = (nty - 8.0f) * g.bsy * fe - (bty - 8.0f) * g.bsy * fs;
-#pragma unroll
-                    for (int j = 0; j < RPL; j++) {
-                        const int row = (lane >> 4) + 2 * j;
-                        const int yc = __shfl_sync(0xffffffffu, ycode, row);
-                        const float dyp = __shfl_sync(0xffffffffu, dyq, row);
-                        const int mi = cx + 16 * (yc & 15);
-                        const bool wrap = wrapx || (yc & 16);
+                    // step): lane l < 16 computes it for row l and publishes it in the
+                    // warp's row table, {dy, 16 * row index + 256 * edge crossed}, rows
+                    // of one parity together, so a lane reads its eight rows (of its
+                    // parity) with four 16-byte loads -- the same operations on the
+                    // same inputs as a per-ray evaluation, done once instead of 16 times.
+                    if (lane < 16) {
+                        const float bty = __fadd_rn(c.y, lx), nty = __fadd_rn(np.y, lx);
+                        const int ycode = (mid_index16(bty, nty) << 4) | (crosses16(bty, nty) ? 256 : 0);
+                        const float dyq = (nty - 8.0f) * g.bsy * fe - (bty - 8.0f) * g.bsy * fs;
+                        ytab[(lane & 1) * 8 + (lane >> 1)] = make_float2(dyq, __int_as_float(ycode));
+                    }
+                    __syncwarp();
+                    const float4* yrow = reinterpret_cast<const float4*>(ytab) + 4 * (lane >> 4);
+                    // ray j of this lane: row (lane >> 4) + 2 j
+                    auto ray = [&](int j, float dyp, int yc) {
+                        const int mi = cx | (yc & 0xf0);
+                        const bool wrap = ((yc | wx) & 256) != 0;
                         const float l2 = dxz2 + dyp * dyp;
                         const float len = seg_length(l2);
-                        const float2 trv = tr[mi];
-                        const float p = len * trv.y;
+                        const float4 e = mywb[mi];  // Terma, density, dose, path sum
+                        const float p = len * e.y;
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
-                        float2 acc = mydp[mi];
-                        acc.x += dep;
-                        acc.y += p;
-                        mydp[mi] = acc;
-                        XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
-                        XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
+                        *reinterpret_cast<float2*>(&mywb[mi].z) = make_float2(e.z + dep, e.w + p);
+                        XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - e.x, e.x);
+                        XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - e.x, e.x);
+                    };
+#pragma unroll
+                    for (int q = 0; q < RPL / 2; q++) {
+                        const float4 y2 = yrow[q];
+                        ray(2 * q, y2.x, __float_as_int(y2.y));
+                        ray(2 * q + 1, y2.z, __float_as_int(y2.w));
                     }
                 } else if constexpr (kCols) {
                     const float btx = __fadd_rn(c.x, fcol), ntx = __fadd_rn(np.x, fcol);
@@ -371,9 +398,15 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || 
             const int s_new = *s_abort ? g.L : *s_next;
             // reduce azimuths in order; normalise by the last azimuth's path sum
             for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
-                float sum = 0.0f;
-                for (int w = 0; w < n_phi; w++) sum += dp[(size_t)w * g.P + v].x;
-                const float val = sum / (dp[(size_t)(n_phi - 1) * g.P + v].y + 1e-4f);
+                float sum = 0.0f, last_sum_p;
+                if constexpr (kFx16) {
+                    for (int w = 0; w < n_phi; w++) sum += wb[(size_t)w * g.P + v].z;
+                    last_sum_p = wb[(size_t)(n_phi - 1) * g.P + v].w;
+                } else {
+                    for (int w = 0; w < n_phi; w++) sum += dp[(size_t)w * g.P + v].x;
+                    last_sum_p = dp[(size_t)(n_phi - 1) * g.P + v].y;
+                }
+                const float val = sum / (last_sum_p + 1e-4f);
                 if (split)
                     split_out[(size_t)blockIdx.x * split_stride + (size_t)s * g.P + v] = val;
                 else
@@ -382,10 +415,9 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 || 
                     // without waiting for D's old value
                     atomicAdd(D + (size_t)s * pitch + v, val);
             }
-            __syncthreads();  // dp and tr are read; s_next was read by every thread
+            __syncthreads();  // the sums and the slice are read; s_next was read by every thread
             s = s_new;
         }
-        (void)last_phi;
     }
 }
 
@@ -429,8 +461,8 @@ int launch_march(int map, int maxP, int n_phi, unsigned blocks, cudaStream_t st,
     const size_t shm = (size_t)(1 + n_phi) * maxP * sizeof(float2);
     const bool warps_ok = threads >= 128 && threads <= kFx16Threads;
     if (map == 16 && threads <= kFx16Threads)
-        return launch_instance<8, true, false>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
-                                               plane_stride, status);
+        return launch_instance<8, true, false>(blocks, threads, (size_t)n_phi * (256 * sizeof(float4) + 16 * sizeof(float2)),
+                                               st, d_beams, T, R, D, dirs, cp, split, planes, plane_stride, status);
     if (map > 0 && map <= 32 && warps_ok) {
         const int k = 32 / map, rows = (map + k - 1) / k;  // rows per lane
         if (rows <= 8)
