@@ -41,10 +41,9 @@ namespace fd2 {
 namespace {
 
 constexpr int kStepCap = 1 << 20;  // per-slice step cap (the watchdog bound)
-// The 16x16 march is compiled for at most 8 azimuth warps and 5 such blocks
-// of 256 threads per SM (48 registers a thread), i.e. 7 blocks of 192 threads:
-// more resident azimuth warps hide the march's dependency chains and the
-// per-slice barrier (measured faster than 64 registers at 5 blocks of 192).
+// The 16x16 march is compiled for at most 8 azimuth warps (register budget
+// for 4 such blocks of 256 threads, i.e. 5 blocks of 192 threads, per SM;
+// measured faster than 48 registers at 7 blocks of 192).
 constexpr int kFx16Threads = 256;
 
 struct RayGeom {  // per-beamlet scalars the march needs
@@ -55,20 +54,50 @@ struct RayGeom {  // per-beamlet scalars the march needs
     int fx, fy, P, L;
 };
 
-__device__ __forceinline__ float step_to_boundary(float c, float d) {
-    // (ceil(c + 1e-3) - c) / d for d > 0, (floor(c - 1e-3) - c) / d otherwise,
-    // with the reference's fast division (its build uses -use_fast_math, whose
-    // a/b is bitwise __fdividef(a, b)).  An axis the ray does not move along
-    // never limits the step (the reference divides by zero there and the ray
-    // becomes NaN and never ends its slice).
-    if (d == 0.0f) return __int_as_float(0x7f800000);
-    return d > 0.0f ? __fdividef(__fsub_rn(ceilf(__fadd_rn(c, 1e-3f)), c), d)
-                    : __fdividef(__fsub_rn(floorf(__fsub_rn(c, 1e-3f)), c), d);
+// 1/x on the special-function unit (PTX rcp.approx.ftz.f32).
+__device__ __forceinline__ float rcp_sfu(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// A cone direction with what the boundary step needs of it, formed once per
+// (zenith, azimuth) pass: the sign of each component and the reciprocal of its
+// magnitude (+inf for a zero component).
+struct ConeDir {
+    float3 d, sg, ra;
+};
+
+__device__ __forceinline__ ConeDir make_cone_dir(float3 d) {
+    ConeDir k;
+    k.d = d;
+    k.sg = make_float3(d.x < 0.0f ? -1.0f : 1.0f, d.y < 0.0f ? -1.0f : 1.0f, d.z < 0.0f ? -1.0f : 1.0f);
+    k.ra = make_float3(rcp_sfu(fabsf(d.x)), rcp_sfu(fabsf(d.y)), rcp_sfu(fabsf(d.z)));
+    return k;
+}
+
+// The reference's step to the next boundary along one axis (its build uses
+// -use_fast_math, whose a/b is a * rcp.approx(b)):
+//     (ceil(c + 1e-3) - c) / d    for d > 0,
+//     (floor(c - 1e-3) - c) / d   otherwise.
+// With s = sign(d) and u = s c (exact), floor(c - 1e-3) - c = -(ceil(u + 1e-3) - u)
+// (round-to-nearest is symmetric under negation) and the sign cancels against
+// d's, so both cases are (ceil(u + 1e-3) - u) * rcp(|d|): one rounding
+// function and no division per step.  u + 1e-3 and ceil(...) - u are single
+// fused operations on the exact product s c, so they round as the
+// reference's additions do.  A zero component gives rcp(0) = +inf, so an axis
+// the ray does not move along never limits the step (the reference divides
+// by zero there and the ray becomes NaN and never ends its slice).
+__device__ __forceinline__ float step_to_boundary(float c, float s, float ra) {
+    const float up = ceilf(__fmaf_rn(c, s, 1e-3f));
+    return __fmul_rn(__fmaf_rn(-c, s, up), ra);
 }
 
 // d_nextPoint (DoseComp.cu:76-111): the next voxel-boundary point of the base ray.
-__device__ __forceinline__ bool next_point(float3 c, float3 d, float3& np) {
-    float sx = step_to_boundary(c.x, d.x), sy = step_to_boundary(c.y, d.y), sz = step_to_boundary(c.z, d.z);
+__device__ __forceinline__ bool next_point(float3 c, const ConeDir& k, float3& np) {
+    const float3 d = k.d;
+    float sx = step_to_boundary(c.x, k.sg.x, k.ra.x), sy = step_to_boundary(c.y, k.sg.y, k.ra.y),
+          sz = step_to_boundary(c.z, k.sg.z, k.ra.z);
     float take = fminf(fminf(sx, sy), sz);
     np = make_float3(__fmaf_rn(take, d.x, c.x), __fmaf_rn(take, d.y, c.y), __fmaf_rn(take, d.z, c.z));
     bool flag = fabsf(__fsub_rn(np.z, roundf(np.z))) < 1e-4f;
@@ -148,7 +177,7 @@ __device__ __forceinline__ float seg_length(float l2) {
 // row and shared by shuffles (16 x 16 maps share it through the row table);
 // RPL >= ceil(F / k).
 template <int RPL, bool kFx16, bool kCols = false>
-__global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 5 : ((kCols && RPL <= 8) ? 4 : (kCols ? 3 : 1)))
+__global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 4 : ((kCols && RPL <= 8) ? 4 : (kCols ? 3 : 1)))
     cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
@@ -224,8 +253,9 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 5
         const float Aa = cp.A_a[t], Bb = cp.B_b[t];
         const float ka = -cp.a[t] * 1.4426950408889634f, kb = -cp.b[t] * 1.4426950408889634f;  // -k log2(e)
         const float4 d4 = dirs[((size_t)bi * n_tf + t) * n_phi + warp];
-        const float3 d = make_float3(d4.x, d4.y, d4.z);
+        const ConeDir cd = make_cone_dir(make_float3(d4.x, d4.y, d4.z));
         float3 c = make_float3(0.5f, 0.5f, 0.0f);
+        float fs = (c.z * g.ls + g.lim_min) * g.inv_sad;  // divergence factor at c, carried step to step
         float XA[RPL], XB[RPL];
 #pragma unroll
         for (int j = 0; j < RPL; j++) XA[j] = XB[j] = 0.0f;
@@ -271,44 +301,49 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 5
             int guard = 0;
             for (;;) {
                 float3 np;
-                const bool flag = next_point(c, d, np);
+                const bool flag = next_point(c, cd, np);
                 const float fe = (np.z * g.ls + g.lim_min) * g.inv_sad;
-                const float fs = (c.z * g.ls + g.lim_min) * g.inv_sad;
                 const float dzp = (np.z - c.z) * g.ls;
                 if constexpr (kFx16) {
-                    // 16x16 map: a lane's rays share their column, so the x half of
-                    // the voxel/edge/length work is done once per lane per step
+                    // 16x16 map.  A lane's rays share their column, and the rays of
+                    // one row share their row: the voxel/edge/length work splits into
+                    // an x half per column and a y half per row, 16 of each per step.
+                    // Lanes 0-15 evaluate the x half of column `lane`, lanes 16-31 the
+                    // y half of row `lane - 16`, in the same instructions (the same
+                    // operations on the same inputs as a per-ray evaluation, done once
+                    // per column or row instead of per ray).  The half's edge
+                    // crossing travels as the sign bit of its |offset|, which enters
+                    // the length only squared.  Rows go to the warp's row table
+                    // {+-|dy|, 256 * row} (bytes into the slice copy), rows of one
+                    // parity together, so a lane reads its eight rows (of its parity)
+                    // with four 16-byte loads; lanes 16-31 take their column's x half
+                    // from lanes 0-15 by shuffle.
                     const float lx = (float)(lane & 15);
-                    const float btx = __fadd_rn(c.x, lx), ntx = __fadd_rn(np.x, lx);
-                    const int cx = mid_index16(btx, ntx);
-                    const int wx = crosses16(btx, ntx) ? 256 : 0;
-                    const float dxp = (ntx - 8.0f) * g.bsx * fe - (btx - 8.0f) * g.bsx * fs;
-                    const float dxz2 = dxp * dxp + dzp * dzp;
-                    // The y half depends only on the ray's row offset (16 values per
-                    // step): lane l < 16 computes it for row l and publishes it in the
-                    // warp's row table, {dy, 16 * row index + 256 * edge crossed}, rows
-                    // of one parity together, so a lane reads its eight rows (of its
-                    // parity) with four 16-byte loads -- the same operations on the
-                    // same inputs as a per-ray evaluation, done once instead of 16 times.
-                    if (lane < 16) {
-                        const float bty = __fadd_rn(c.y, lx), nty = __fadd_rn(np.y, lx);
-                        const int ycode = (mid_index16(bty, nty) << 4) | (crosses16(bty, nty) ? 256 : 0);
-                        const float dyq = (nty - 8.0f) * g.bsy * fe - (bty - 8.0f) * g.bsy * fs;
-                        ytab[(lane & 1) * 8 + (lane >> 1)] = make_float2(dyq, __int_as_float(ycode));
-                    }
+                    const bool yl = lane >= 16;
+                    const float hb = __fadd_rn(yl ? c.y : c.x, lx), hn = __fadd_rn(yl ? np.y : np.x, lx);
+                    const float bs = yl ? g.bsy : g.bsx;
+                    const int hi = mid_index16(hb, hn);
+                    const float hq = fabsf((hn - 8.0f) * bs * fe - (hb - 8.0f) * bs * fs);
+                    const float hs = crosses16(hb, hn) ? -hq : hq;
+                    if (yl) ytab[(lane & 1) * 8 + ((lane & 15) >> 1)] = make_float2(hs, __int_as_float(hi << 8));
+                    const int cx = __shfl_sync(0xffffffffu, hi, lane & 15);
+                    const float dxs = __shfl_sync(0xffffffffu, hs, lane & 15);
+                    const float dxz2 = dxs * dxs + dzp * dzp;
+                    const int wx = __float_as_int(dxs);
+                    const char* col = reinterpret_cast<const char*>(mywb) + (cx << 4);
                     __syncwarp();
                     const float4* yrow = reinterpret_cast<const float4*>(ytab) + 4 * (lane >> 4);
                     // ray j of this lane: row (lane >> 4) + 2 j
-                    auto ray = [&](int j, float dyp, int yc) {
-                        const int mi = cx | (yc & 0xf0);
-                        const bool wrap = ((yc | wx) & 256) != 0;
-                        const float l2 = dxz2 + dyp * dyp;
+                    auto ray = [&](int j, float dys, int yoff) {
+                        const bool wrap = (__float_as_int(dys) | wx) < 0;
+                        const float l2 = dxz2 + dys * dys;
                         const float len = seg_length(l2);
-                        const float4 e = mywb[mi];  // Terma, density, dose, path sum
+                        float4* v = const_cast<float4*>(reinterpret_cast<const float4*>(col + yoff));
+                        const float4 e = *v;  // Terma, density, dose, path sum
                         const float p = len * e.y;
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
-                        *reinterpret_cast<float2*>(&mywb[mi].z) = make_float2(e.z + dep, e.w + p);
+                        *reinterpret_cast<float2*>(&v->z) = make_float2(e.z + dep, e.w + p);
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - e.x, e.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - e.x, e.x);
                     };
@@ -379,6 +414,7 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 5
                 }
                 }
                 c = np;
+                fs = fe;
                 __syncwarp();
                 if (flag) break;
                 if (++guard >= kStepCap) {
