@@ -104,9 +104,14 @@ __device__ __forceinline__ bool candidate(const ColumnInfo& ci, float3 c, float 
 // farther than extent + hdiag from the beamlet axis.  Sample positions are
 // affine in the sub-sample indices, so the beam-frame coordinates are stepped
 // incrementally; one reciprocal of the depth per sample gives the divergent
-// lateral scale; consecutive samples that land in the same texel reuse it.
+// lateral scale.  SS > 0: ss == SS known at compile time, the innermost line
+// of samples unrolled -- independent samples whose loads are predicated
+// rather than branched around; SS == 0: any ss, consecutive samples that land
+// in the same texel reuse it.  Both add the same values in the same order.
+template <int SS>
 __device__ __forceinline__ float column_value(const ColumnInfo& ci, const float* __restrict__ bev, int x, int y,
-                                              int z, float3 vs, float hdiag, float extent, int ss) {
+                                              int z, float3 vs, float hdiag, float extent, int ss_rt) {
+    const int ss = SS > 0 ? SS : ss_rt;
     const float3 c = make_float3((x + 0.5f) * vs.x, (y + 0.5f) * vs.y, (z + 0.5f) * vs.z);
     const float3 v = rot(ci.R, make_float3(c.x - ci.src[0], c.y - ci.src[1], c.z - ci.src[2]));
     if (sqrtf(v.x * v.x + v.z * v.z) > hdiag + extent) return 0.0f;
@@ -127,20 +132,34 @@ __device__ __forceinline__ float column_value(const ColumnInfo& ci, const float*
         const float3 uk = make_float3(u0.x + kk * dK.x, u0.y + kk * dK.y, u0.z + kk * dK.z);
         for (int jj = 0; jj < ss; jj++) {
             const float3 ukj = make_float3(uk.x + jj * dJ.x, uk.y + jj * dJ.y, uk.z + jj * dJ.z);
-            for (int ii = 0; ii < ss; ii++) {
-                const float ux = ukj.x + ii * dI.x, uy = ukj.y + ii * dI.y, uz = ukj.z + ii * dI.z;
-                const float r = __fdividef(1.0f, uy);
-                const float cnx = ux * r * sx + ci.hx, cnz = uz * r * sz + ci.hy;
-                if (cnx < 0.0f || cnx > ffx || cnz < 0.0f || cnz > ffy) continue;
-                const int tx = __float2int_rd(cnx), ty = __float2int_rd(cnz);
-                const int tz = __float2int_rd((uy - ci.lim_min) * ci.inv_ls);
-                if (tx >= ci.fx || ty >= ci.fy || (unsigned)tz >= (unsigned)ci.L) continue;
-                const int idx = tx + ci.fx * ty + plane * tz;
-                if (idx != last) {
-                    last = idx;
-                    last_v = __ldg(bev + idx);
+            if constexpr (SS > 0) {
+#pragma unroll
+                for (int ii = 0; ii < SS; ii++) {
+                    const float ux = ukj.x + ii * dI.x, uy = ukj.y + ii * dI.y, uz = ukj.z + ii * dI.z;
+                    const float r = __fdividef(1.0f, uy);
+                    const float cnx = ux * r * sx + ci.hx, cnz = uz * r * sz + ci.hy;
+                    const int tx = __float2int_rd(cnx), ty = __float2int_rd(cnz);
+                    const int tz = __float2int_rd((uy - ci.lim_min) * ci.inv_ls);
+                    const bool in = !(cnx < 0.0f || cnx > ffx || cnz < 0.0f || cnz > ffy) && tx < ci.fx &&
+                                    ty < ci.fy && (unsigned)tz < (unsigned)ci.L;
+                    if (in) acc += __ldg(bev + (tx + ci.fx * ty + plane * tz));
                 }
-                acc += last_v;
+            } else {
+                for (int ii = 0; ii < ss; ii++) {
+                    const float ux = ukj.x + ii * dI.x, uy = ukj.y + ii * dI.y, uz = ukj.z + ii * dI.z;
+                    const float r = __fdividef(1.0f, uy);
+                    const float cnx = ux * r * sx + ci.hx, cnz = uz * r * sz + ci.hy;
+                    if (cnx < 0.0f || cnx > ffx || cnz < 0.0f || cnz > ffy) continue;
+                    const int tx = __float2int_rd(cnx), ty = __float2int_rd(cnz);
+                    const int tz = __float2int_rd((uy - ci.lim_min) * ci.inv_ls);
+                    if (tx >= ci.fx || ty >= ci.fy || (unsigned)tz >= (unsigned)ci.L) continue;
+                    const int idx = tx + ci.fx * ty + plane * tz;
+                    if (idx != last) {
+                        last = idx;
+                        last_v = __ldg(bev + idx);
+                    }
+                    acc += last_v;
+                }
             }
         }
     }
@@ -240,7 +259,8 @@ __global__ void __launch_bounds__(kColThreads) column_value_kernel(
         for (uint32_t k = threadIdx.x; k < pend; k += kColThreads) {
             const int v = s_cand[k];
             const int x = v % nx, y = (v / nx) % ny, z = v / (nx * ny);
-            s_val[k] = column_value(ci, bev, x, y, z, vs, hdiag, extent, ss);
+            s_val[k] = ss == 5 ? column_value<5>(ci, bev, x, y, z, vs, hdiag, extent, ss)
+                               : column_value<0>(ci, bev, x, y, z, vs, hdiag, extent, ss);
         }
         __syncthreads();
         const uint32_t per = (pend + kColThreads - 1) / kColThreads;  // a contiguous run per thread
