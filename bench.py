@@ -12,7 +12,8 @@ stage into the per-beam CSR dose-loading matrices, all beams in one call.
 One JSON line on rank 0.  `value` is device-timed with the density resident in
 HBM; `e2e` goes through the public API with host inputs (density volume and
 beamlet descriptors copied from pinned memory every step) and the whole CSR
-result read back into pinned memory.  Multi-GPU: one process per GPU; N GPUs
+result read back into pinned memory, batch by batch while the next batch is
+computed (DoseMatConstruction's host_out).  Multi-GPU: one process per GPU; N GPUs
 take a 4pi candidate set of N x 400 beams, partitioned by beam across the
 ranks by a greedy balance on the CCCS march length (fastdose_b200.sharding),
 each rank building its share's matrices with no collective on the data path;
@@ -188,14 +189,6 @@ def _bundle_beam(bb):
     b["angles"] = bb["angles"]
     b["long_spacing"] = bb["long_spacing"]
     return b
-
-
-class _DevView:
-    """Zero-copy device view (for torch) of a raw CUDA pointer."""
-
-    def __init__(self, ptr, n, typestr):
-        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False), "version": 3,
-                                         "strides": None}
 
 
 def time_spmv(M, n_in, n_out, peak, reps=10, warmup=3):
@@ -670,22 +663,20 @@ def run_fd2(args, rank, world):
         o += len(b)
     dens_np = dens_host.numpy().reshape(ph.density.shape)
 
+    # The matrix comes back to pinned host buffers while it is built: each
+    # batch's rows are copied on a copy stream during the next batch's device
+    # work (host_out), so only the last batch's copy follows the construction.
+    host = api.HostCSR(n_bl, info["nnz"])
+    e2e_batch = args.e2e_batch if args.e2e_batch >= 0 else max(4096, -(-n_bl // 6))
+
     def step_e2e():
         # the library copies the density volume and the beamlet descriptors from these pinned host buffers
         dn = api.Density(ctx, dens_np, ph.volume)
-        m = api.DoseMatConstruction(ctx, per, fluence, dn, spec, kern, stream=stream)
-        inf = m.info()
-        ro, col, val, _ = m.device_views()
-        outs = [(ro, inf["n_rows"] + 1, "<i8"), (col, inf["nnz"], "<i4"), (val, inf["nnz"], "<f4")]
-        nbytes = 0
-        for ptr, n, ts in outs:
-            src = torch.as_tensor(_DevView(ptr, n, ts), device="cuda")
-            dst = torch.empty(n, dtype=src.dtype, pin_memory=True)
-            dst.copy_(src, non_blocking=True)
-            nbytes += dst.numel() * dst.element_size()
-        torch.cuda.current_stream().synchronize()
+        m = api.DoseMatConstruction(ctx, per, fluence, dn, spec, kern, stream=stream, host_out=host,
+                                    batch_beamlets=e2e_batch)
         m.close()
-        return nbytes
+        dn.close()
+        return host.nbytes()
 
     for _ in range(max(1, min(args.warmup, 2))):
         d2h = step_e2e()
@@ -759,7 +750,8 @@ def run_fd2(args, rank, world):
                               "frac": pipe_bytes / (pipe_ms * 1e-3) / 1e9 / peak,
                               "basis": "per beamlet 4 P L 6 + 4 per footprint voxel (taken as its nonzeros) + "
                                        "8 per nonzero (value, index) + 8 per row offset"},
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "batch_beamlets": int(e2e_batch), "read_back": "pinned, overlapped with the next batch"},
         "clocks": clk_now,
     }
     if not args.no_extras:
@@ -791,6 +783,8 @@ def main():
                     help="time A x and A^T y of the optimization matrix in one format (profiling)")
     ap.add_argument("--spmv-reps", type=int, default=10)
     ap.add_argument("--served-workers", type=int, default=2)
+    ap.add_argument("--e2e-batch", type=int, default=-1,
+                    help="beamlets per construction batch of the end-to-end leg (-1: a sixth of the plan, >= 4096)")
     ap.add_argument("--c4", action="store_true", help="run the multi-isocentre configuration alone")
     ap.add_argument("--only-served", action="store_true", help="run the served leg alone")
     args = ap.parse_args()

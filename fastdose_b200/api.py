@@ -285,7 +285,7 @@ def BEV2PVCSInterp(ctx, batch, beamlets_per_beam, density, extent=2.0, ss_factor
     `batch` (a BEVBatch whose beams are the concatenation of beamlets_per_beam)."""
     counts = np.array(beamlets_per_beam, np.uint32)
     assert counts.sum() == len(batch.beams)
-    prm = _Params(extent, ss_factor, VALUE_TYPES[value_type], -1, 0, 0, 0)
+    prm = _Params(extent, ss_factor, VALUE_TYPES[value_type], -1, 0, 0, 0, None)
     h = C.c_void_p()
     _lib.check(ctx.lib.fd2_bev2pvcs_interp(ctx.h, len(counts), _p(counts), _p(batch.beams), batch.ptrs("dose"),
                                            density.h, C.byref(prm), C.byref(h),
@@ -327,7 +327,52 @@ def beamletFlagInit(ctx, bundles, ptv_mask, volume, super_sampling=3):
 # ------------------------------------------------------------------ dose matrix
 class _Params(C.Structure):
     _fields_ = [("extent", C.c_float), ("ss_factor", C.c_int), ("value_type", C.c_int), ("cccs_schedule", C.c_int),
-                ("batch_beamlets", C.c_uint64), ("memory_budget", C.c_uint64), ("verbose", C.c_int)]
+                ("batch_beamlets", C.c_uint64), ("memory_budget", C.c_uint64), ("verbose", C.c_int),
+                ("host_out", C.c_void_p)]
+
+
+class _HostCSR(C.Structure):
+    _fields_ = [("row_off", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p), ("scale", C.c_void_p),
+                ("cap_nnz", C.c_uint64), ("nnz", C.c_uint64)]
+
+
+class HostCSR:
+    """Pinned host buffers a dose matrix is copied into while it is built
+    (fd2_host_csr_t): DoseMatConstruction(..., host_out=this) copies each
+    finished batch of rows on a copy stream while the device computes the next
+    batch.  Reusable across constructions of up to `n_rows` rows and `cap_nnz`
+    nonzeros."""
+
+    def __init__(self, n_rows, cap_nnz, value_type="f32"):
+        torch = _torch()
+        self.value_type = value_type
+        vt = torch.float32 if value_type == "f32" else torch.int16
+        self.row_off = torch.empty(int(n_rows) + 1, dtype=torch.int64, pin_memory=True)
+        self.col = torch.empty(max(1, int(cap_nnz)), dtype=torch.int32, pin_memory=True)
+        self.val = torch.empty(max(1, int(cap_nnz)), dtype=vt, pin_memory=True)
+        self.scale = torch.empty(max(1, int(n_rows)), dtype=torch.float32, pin_memory=True)
+        self.cap_nnz = int(cap_nnz)
+        self.n_rows = 0
+        self.nnz = 0
+
+    def _struct(self):
+        return _HostCSR(self.row_off.data_ptr(), self.col.data_ptr(), self.val.data_ptr(), self.scale.data_ptr(),
+                        self.cap_nnz, 0)
+
+    def arrays(self):
+        """(row_off, col, val) of the last matrix copied in, as numpy views
+        (val: float32, or the raw 16-bit words of an f16/bf16 matrix), plus the
+        row scales for 16-bit values (None for f32)."""
+        ro = self.row_off.numpy()[: self.n_rows + 1]
+        col = self.col.numpy()[: self.nnz]
+        val = self.val.numpy()[: self.nnz]
+        sc = None if self.value_type == "f32" else self.scale.numpy()[: self.n_rows]
+        return ro, col, val, sc
+
+    def nbytes(self):
+        vb = 4 if self.value_type == "f32" else 2
+        n = (self.n_rows + 1) * 8 + self.nnz * (4 + vb)
+        return n + (self.n_rows * 4 if self.value_type != "f32" else 0)
 
 
 class _Info(C.Structure):
@@ -406,18 +451,30 @@ class MatCSREnsemble:
 
 def DoseMatConstruction(ctx, beamlets_per_beam, fluence, density, spectrum, kernel, extent=2.0, ss_factor=5,
                         value_type="f32", cccs_schedule=-1, memory_budget=0, batch_beamlets=0, verbose=False,
-                        stream=None):
+                        stream=None, host_out=None):
     """IMRT::DoseMatConstruction: `beamlets_per_beam` is a list of BEAM_DTYPE
-    arrays (one per beam).  Returns a MatCSREnsemble."""
+    arrays (one per beam).  Returns a MatCSREnsemble.  host_out: a HostCSR
+    (of this value type) that receives a host copy of the matrix, batch by
+    batch while it is built."""
     counts = np.array([len(b) for b in beamlets_per_beam], np.uint32)
     allb = np.ascontiguousarray(np.concatenate([np.asarray(b, BEAM_DTYPE).reshape(-1) for b in beamlets_per_beam]),
                                 BEAM_DTYPE) if len(beamlets_per_beam) else np.zeros(0, BEAM_DTYPE)
     fl = np.ascontiguousarray(fluence, np.float32)
+    hs = None
+    if host_out is not None:
+        if host_out.value_type != value_type:
+            raise ValueError(f"host_out holds {host_out.value_type} values, the matrix is {value_type}")
+        if host_out.row_off.numel() < allb.size + 1:
+            raise ValueError(f"host_out holds {host_out.row_off.numel() - 1} rows, the plan has {allb.size}")
+        hs = host_out._struct()
     prm = _Params(extent, ss_factor, VALUE_TYPES[value_type], cccs_schedule, batch_beamlets, memory_budget,
-                  int(verbose))
+                  int(verbose), C.cast(C.pointer(hs), C.c_void_p) if hs is not None else None)
     h = C.c_void_p()
     st = ctx.lib.fd2_dose_mat_construct(ctx.h, len(counts), _p(counts), _p(allb), _p(fl), density.h, spectrum.h,
                                         kernel.h, C.byref(prm), C.byref(h),
                                         _stream_ptr(stream) if stream is not None else None)
     _lib.check(st, "dose_mat_construct")
+    if host_out is not None:
+        host_out.n_rows = int(allb.size)
+        host_out.nnz = int(hs.nnz)
     return MatCSREnsemble(ctx, h)

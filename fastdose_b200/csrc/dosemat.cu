@@ -291,6 +291,95 @@ static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const 
     return rc;
 }
 
+// The host copy of a matrix under construction (fd2_dosemat_params_t.host_out).
+// After the device work of batch k is enqueued, batch k-1's rows are copied
+// to the caller's buffers on a copy stream, so the copy runs while the device
+// computes batch k; only the last batch's copy follows the construction.  The
+// size of a batch's nonzero range is read from its own row offsets, which go
+// to the caller's row_off buffer first: the host waits for them (by then the
+// device is busy with the next batch) and then issues the column and value
+// copies of exactly that range.
+struct HostSink {
+    struct Batch {
+        uint64_t row0 = 0, row1 = 0;
+        cudaEvent_t offsets = nullptr;  // on the copy stream: the batch's row offsets are on the host
+    };
+    fd2_host_csr_t* out = nullptr;
+    fd2_csr_ensemble* e = nullptr;
+    cudaStream_t cs = nullptr;
+    bool have_pending = false;
+    Batch pending;
+
+    int init(fd2_host_csr_t* o, fd2_csr_ensemble* ens, uint64_t n_rows) {
+        FD2_REQUIRE(o->row_off && o->col && o->val, FD2_ERR_INVALID_ARGUMENT,
+                    "dose_mat_construct: host_out needs row_off, col and val");
+        FD2_REQUIRE(ens->value_type == FD2_VALUES_F32 || o->scale, FD2_ERR_INVALID_ARGUMENT,
+                    "dose_mat_construct: host_out of a 16-bit matrix needs scale");
+        out = o;
+        e = ens;
+        out->nnz = 0;
+        out->row_off[0] = 0;
+        (void)n_rows;
+        FD2_CHECK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        return FD2_OK;
+    }
+    // rows [row0, row1) are enqueued on st
+    int batch_done(uint64_t row0, uint64_t row1, cudaStream_t st) {
+        if (have_pending) FD2_TRY(flush());
+        cudaEvent_t done = nullptr;
+        FD2_CHECK_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+        cudaError_t err = cudaEventRecord(done, st);
+        if (err == cudaSuccess) err = cudaStreamWaitEvent(cs, done, 0);
+        cudaEventDestroy(done);  // released once it has completed
+        FD2_CHECK_CUDA(err);
+        FD2_CHECK_CUDA(cudaMemcpyAsync(out->row_off + row0 + 1, e->d_row_off + row0 + 1,
+                                       (row1 - row0) * sizeof(int64_t), cudaMemcpyDeviceToHost, cs));
+        pending = Batch{row0, row1, nullptr};
+        FD2_CHECK_CUDA(cudaEventCreateWithFlags(&pending.offsets, cudaEventDisableTiming));
+        have_pending = true;
+        FD2_CHECK_CUDA(cudaEventRecord(pending.offsets, cs));
+        return FD2_OK;
+    }
+    int flush() {
+        have_pending = false;
+        const Batch b = pending;
+        cudaError_t err = cudaEventSynchronize(b.offsets);
+        cudaEventDestroy(b.offsets);
+        FD2_CHECK_CUDA(err);
+        const uint64_t s0 = (uint64_t)out->row_off[b.row0], s1 = (uint64_t)out->row_off[b.row1];
+        FD2_REQUIRE(s1 <= out->cap_nnz, FD2_ERR_CAPACITY,
+                    "dose_mat_construct: host_out holds %llu nonzeros, the matrix has at least %llu",
+                    (unsigned long long)out->cap_nnz, (unsigned long long)s1);
+        const size_t vb = value_bytes(e->value_type);
+        if (s1 > s0) {
+            FD2_CHECK_CUDA(cudaMemcpyAsync(out->col + s0, e->d_col + s0, (s1 - s0) * sizeof(int32_t),
+                                           cudaMemcpyDeviceToHost, cs));
+            FD2_CHECK_CUDA(cudaMemcpyAsync((char*)out->val + s0 * vb, (const char*)e->d_val + s0 * vb,
+                                           (s1 - s0) * vb, cudaMemcpyDeviceToHost, cs));
+        }
+        if (e->value_type != FD2_VALUES_F32 && b.row1 > b.row0)
+            FD2_CHECK_CUDA(cudaMemcpyAsync(out->scale + b.row0, e->d_scale + b.row0, (b.row1 - b.row0) * sizeof(float),
+                                           cudaMemcpyDeviceToHost, cs));
+        out->nnz = s1;
+        return FD2_OK;
+    }
+    int finish() {
+        if (have_pending) FD2_TRY(flush());
+        FD2_CHECK_CUDA(cudaStreamSynchronize(cs));
+        return FD2_OK;
+    }
+    void drain() {
+        if (cs) cudaStreamSynchronize(cs);
+    }
+    ~HostSink() {
+        if (have_pending) cudaEventDestroy(pending.offsets);
+        if (cs) {
+            cudaStreamSynchronize(cs);  // no copy may outlive the ensemble's arrays
+            cudaStreamDestroy(cs);
+        }
+    }
+};
+
 }  // namespace fd2
 
 using namespace fd2;
@@ -306,6 +395,7 @@ void fd2_dosemat_params_default(fd2_dosemat_params_t* p) {
     p->batch_beamlets = 0;
     p->memory_budget = 0;
     p->verbose = 0;
+    p->host_out = nullptr;
 }
 
 int fd2_bev2pvcs(fd2_context* ctx, const fd2_beam_t* h_beam, const fd2_density* density, const float* d_bev,
@@ -383,6 +473,8 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     uint64_t cap_total = 0;
     for (uint32_t c : cnt) cap_total += c;
     if (!rc) rc = ensemble_reserve(e, total, cap_total);
+    HostSink sink;  // declared before the ensemble is destroyed on any path: its copies finish first
+    if (!rc && params.host_out) rc = sink.init(params.host_out, e, total);
     if (rc) {
         if (d_infos) cudaFreeAsync(d_infos, st);
         fd2_csr_ensemble_destroy(e);
@@ -469,6 +561,10 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         for (void* p : {(void*)aF, (void*)aT, (void*)aR, (void*)aD})  // d_bev is the context's
             if (p) cudaFreeAsync(p, st);
         if (rc) break;
+        if (params.host_out) {
+            rc = sink.batch_done(e->n_rows - nb, e->n_rows, st);
+            if (rc) break;
+        }
         // per-beam row boundaries
         size_t row = e->n_rows - nb;
         for (size_t i = beam0; i < beam1; i++) {
@@ -486,6 +582,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     if (d_infos) cudaFreeAsync(d_infos, st);
     if (!rc) rc = ensemble_sync_nnz(e);  // the one wait of the construction, besides the candidate counts
     cudaStreamSynchronize(st);
+    if (!rc && params.host_out) rc = sink.finish();
     if (!rc) {
         fd2::DeviceStatus ds;
         if (cudaMemcpy(&ds, ctx->d_status, sizeof(ds), cudaMemcpyDeviceToHost) == cudaSuccess && ds.code != 0) {
@@ -495,6 +592,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         }
     }
     if (rc) {
+        sink.drain();  // copies still reading the ensemble end before its arrays are freed
         fd2_csr_ensemble_destroy(e);
         return rc;
     }

@@ -226,6 +226,7 @@ int fd2_service_submit(fd2_service* s, const fd2_plan_request_t* q, uint64_t* ti
     r->phi.assign(q->phi, q->phi + q->n_phi);
     r->params = q->params;
     r->params.memory_budget = s->bev_budget;
+    r->params.host_out = nullptr;  // a served request's result stays on the device
     r->stats.beamlets = total;
     r->stats.est_bytes = estimate_bytes(*r, s->bev_budget);
     FD2_REQUIRE(r->stats.est_bytes <= s->budget, FD2_ERR_ADMISSION,

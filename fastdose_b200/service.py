@@ -82,7 +82,7 @@ class Service:
                     (C.c_uint32 * 3)(*vol["bbox_start"]), (C.c_uint32 * 3)(*vol["bbox_dim"]))
         req = _Request(_p(dens), v, len(counts), _p(counts), _p(allb), _p(fl), spectrum.n, *(_p(x) for x in sp),
                        kernel.n_theta, *(_p(x) for x in kn), kernel.n_phi, _p(phi),
-                       _Params(extent, ss_factor, VALUE_TYPES[value_type], -1, 0, 0, 0))
+                       _Params(extent, ss_factor, VALUE_TYPES[value_type], -1, 0, 0, 0, None))
         t = C.c_uint64()
         _lib.check(self.lib.fd2_service_submit(self.h, C.byref(req), C.byref(t)), "service_submit")
         return t.value

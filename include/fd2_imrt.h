@@ -34,6 +34,25 @@ int fd2_beamlet_flags(fd2_context* ctx, size_t n_bundles, const fd2_bundle_t* h_
                       const uint8_t* h_ptv_mask, const fd2_volume_t* volume, int super_sampling,
                       uint8_t* h_flags_out);
 
+/*
+ * Host copy of a dose matrix, filled while the matrix is built (see
+ * fd2_dosemat_params_t.host_out).  The buffers are the caller's; pinned ones
+ * (cudaHostAlloc, cudaHostRegister) let each batch's copy run on a copy stream
+ * while the device computes the next batch, pageable ones give the same
+ * contents without the overlap.  On return row_off[0..n_rows] holds the
+ * matrix's row offsets (row_off[0] = 0), col/val its first nnz nonzeros, and
+ * for 16-bit values scale[0..n_rows) the row scales -- the arrays
+ * fd2_csr_ensemble_device exposes, in the ensemble's value type.
+ */
+typedef struct fd2_host_csr {
+    int64_t* row_off;   /* [n_rows + 1] */
+    int32_t* col;       /* [cap_nnz] voxel indices */
+    void* val;          /* [cap_nnz] values: float, or 16-bit words for FD2_VALUES_F16/BF16 */
+    float* scale;       /* [n_rows] row scales of 16-bit values; not used (may be NULL) for F32 */
+    uint64_t cap_nnz;   /* capacity of col and val in nonzeros; too small -> FD2_ERR_CAPACITY */
+    uint64_t nnz;       /* out: nonzeros written */
+} fd2_host_csr_t;
+
 /* Dose-matrix construction parameters (the getarg reads of
  * IMRT::DoseMatConstruction, IMRTOpt/src/IMRTDoseMat.cu:32,58,80-81). */
 typedef struct fd2_dosemat_params {
@@ -44,6 +63,8 @@ typedef struct fd2_dosemat_params {
     uint64_t batch_beamlets;    /* 0 = auto (memory budget) */
     uint64_t memory_budget;     /* bytes of BEV scratch per batch; 0 = auto */
     int verbose;                /* print per-batch timings to stdout */
+    fd2_host_csr_t* host_out;   /* NULL (default), or host buffers the matrix is copied into
+                                   batch by batch as it is built (fd2_dose_mat_construct only) */
 } fd2_dosemat_params_t;
 
 void fd2_dosemat_params_default(fd2_dosemat_params_t* p);

@@ -226,3 +226,51 @@ def test_dose_matrix_c1_matches_oracle(ctx):
     sel = ref > 0.1 * dmax
     assert np.abs(gpu - ref).max() <= 5e-2 * dmax
     assert np.abs(gpu - ref)[sel].mean() <= 1e-3 * dmax
+
+
+def _decode16(words, scale, ro, vt):
+    w = np.asarray(words).view(np.uint16)
+    v = w.view(np.float16).astype(np.float32) if vt == "f16" else (w.astype(np.uint32) << 16).view(np.float32)
+    rows = np.repeat(np.arange(len(ro) - 1), np.diff(ro))
+    return (v * np.asarray(scale, np.float32)[rows]).astype(np.float32)
+
+
+@pytest.mark.parametrize("vt", ["f32", "f16"])
+def test_host_copy_while_building(ctx, vt):
+    """host_out receives the matrix batch by batch during the construction
+    (small batches force several overlapped copies): the same arrays as the
+    finished ensemble's read-back, bit for bit.  A buffer that is too small
+    is refused with a capacity error and nothing is left in flight."""
+    from fastdose_b200 import _lib
+
+    case = c1_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    beams = [case["beams"][i:i + 10] for i in range(0, len(case["beams"]), 10)]
+    ref = api.DoseMatConstruction(ctx, beams, case["fluence"], dens, sp, kn, value_type=vt)
+    ro_r, col_r, val_r = ref.to_host()
+    nnz = int(ro_r[-1])
+    host = api.HostCSR(len(ro_r) - 1, nnz + 17, value_type=vt)
+    for batch in (0, 16, 33):
+        m = api.DoseMatConstruction(ctx, beams, case["fluence"], dens, sp, kn, value_type=vt, batch_beamlets=batch,
+                                    host_out=host)
+        ro, col, val, sc = host.arrays()
+        assert host.nnz == nnz and host.n_rows == len(ro_r) - 1
+        np.testing.assert_array_equal(ro, ro_r)
+        np.testing.assert_array_equal(col, col_r)
+        if vt == "f32":
+            np.testing.assert_array_equal(val, val_r)
+        else:
+            np.testing.assert_array_equal(_decode16(val, sc, ro, vt), val_r)
+        assert host.nbytes() == (len(ro_r)) * 8 + nnz * (4 + (4 if vt == "f32" else 2)) + \
+            (0 if vt == "f32" else (len(ro_r) - 1) * 4)
+        m.close()
+    small = api.HostCSR(len(ro_r) - 1, nnz // 2, value_type=vt)
+    with pytest.raises(_lib.FD2Error) as e:
+        api.DoseMatConstruction(ctx, beams, case["fluence"], dens, sp, kn, value_type=vt, batch_beamlets=16,
+                                host_out=small)
+    assert "host_out holds" in str(e.value)
+    # the context is still usable
+    again = api.DoseMatConstruction(ctx, beams, case["fluence"], dens, sp, kn, value_type=vt)
+    np.testing.assert_array_equal(again.to_host()[0], ro_r)
+    for mm in (ref, again):
+        mm.close()
