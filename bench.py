@@ -111,7 +111,7 @@ class ClockSampler:
                 pass
         if sm:
             out = {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                   "samples": len(sm)}
+                   "samples": len(sm), "sm_min_mhz": min(sm)}
         return out
 
 
@@ -544,21 +544,26 @@ def served_leg(ctx, rates=(2.0, 10.0), n_requests=16, seed=11, workers=2):
                     time.sleep(delay * 1e-3)
                 tickets[i] = svc.submit(r["phantom"], r["beams"], r["fluence"], spec, kern)
 
-        th = threading.Thread(target=submitter)
-        th.start()
-        th.join()
-        stats = []
-        for t in tickets:
-            m, s = svc.wait(t)
-            m.close()
-            stats.append(s)
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            th = threading.Thread(target=submitter)
+            th.start()
+            th.join()
+            stats = []
+            for t in tickets:
+                m, s = svc.wait(t)
+                m.close()
+                stats.append(s)
         svc.close()
         lat = np.array([s["end_ms"] - s["submit_ms"] for s in stats])
         span_s = (max(s["end_ms"] for s in stats) - min(s["submit_ms"] for s in stats)) * 1e-3
         out[f"rate_{lam:g}_per_s"] = {
             "service": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                         "queue_p50_ms": float(np.percentile([s["start_ms"] - s["submit_ms"] for s in stats], 50)),
-                        "beamlets_per_s": sum(n_bl) / span_s, "workers": workers},
+                        "beamlets_per_s": sum(n_bl) / span_s, "workers": workers,
+                        # per request: beamlets, worker, queue ms, run ms (arrival order)
+                        "requests": [[int(s["beamlets"]), int(s["worker"]), round(s["start_ms"] - s["submit_ms"], 1),
+                                      round(s["end_ms"] - s["start_ms"], 1)] for s in stats],
+                        "clocks": clk.summary()},
             "plain_single_beam": plain}
     return out
 

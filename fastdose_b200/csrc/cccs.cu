@@ -565,7 +565,7 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     size_t plane_stride = (size_t)maxP * maxL;
     size_t plane_bytes = schedule == 1 ? n_beams * fwd.size() * plane_stride * sizeof(float) : 0;
     void* scratch = nullptr;
-    FD2_TRY(ctx_scratch(ctx, dir_bytes + plane_bytes + 256, &scratch));
+    FD2_TRY(ctx_scratch(ctx, dir_bytes + plane_bytes + 256, stream, &scratch));
     float4* d_dirs = (float4*)scratch;
     float* d_planes = (float*)((char*)scratch + ((dir_bytes + 255) / 256) * 256);
     FD2_TRY(launch_cone_dirs(d_beams, n_beams, ang, d_dirs, stream));

@@ -5,16 +5,46 @@
 
 namespace fd2 {
 
-int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, void** out) {
+int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, cudaStream_t st, void** out) {
     FD2_REQUIRE(slot >= 0 && slot < kBufCount, FD2_ERR_INVALID_ARGUMENT, "ctx_buffer: slot %d", slot);
+    // The buffer lives in the order of the stream of its last use.  A use on
+    // another stream first waits for the device: the earlier use may still be
+    // running (and the stream it ran on may no longer exist).
+    if (ctx->buf[slot] && ctx->buf_stream[slot] != st) FD2_CHECK_CUDA(cudaDeviceSynchronize());
     if (bytes > ctx->buf_bytes[slot]) {
-        if (ctx->buf[slot]) FD2_CHECK_CUDA(cudaFree(ctx->buf[slot]));
+        // the larger buffer replaces the old one in this stream's order: work
+        // already enqueued on it reads the old buffer first
+        if (ctx->buf[slot]) FD2_CHECK_CUDA(cudaFreeAsync(ctx->buf[slot], st));
         ctx->buf[slot] = nullptr;
         ctx->buf_bytes[slot] = 0;
-        FD2_CHECK_CUDA(cudaMalloc(&ctx->buf[slot], bytes));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync(&ctx->buf[slot], bytes, ctx->pool, st));
         ctx->buf_bytes[slot] = bytes;
     }
+    ctx->buf_stream[slot] = st;
     *out = ctx->buf[slot];
+    return FD2_OK;
+}
+
+int density_create_pooled(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume,
+                          fd2_density** out) {
+    FD2_REQUIRE(ctx && host_density && volume && out, FD2_ERR_INVALID_ARGUMENT, "density_create: null argument");
+    const size_t nv = (size_t)volume->dim[0] * volume->dim[1] * volume->dim[2];
+    FD2_REQUIRE(nv > 0, FD2_ERR_INVALID_ARGUMENT, "density_create: empty volume");
+    FD2_REQUIRE(volume->voxel_size[0] > 0 && volume->voxel_size[1] > 0 && volume->voxel_size[2] > 0,
+                FD2_ERR_INVALID_ARGUMENT, "density_create: voxel size must be positive");
+    void* p = nullptr;
+    FD2_CHECK_CUDA(cudaMallocFromPoolAsync(&p, nv * sizeof(float), ctx->pool, ctx->stream));
+    const cudaError_t e = cudaMemcpyAsync(p, host_density, nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(p, ctx->stream);
+        FD2_CHECK_CUDA(e);
+    }
+    auto* d = new fd2_density();
+    d->ctx = ctx;
+    d->vol = *volume;
+    d->d_density = (float*)p;
+    d->pooled = true;
+    *out = d;
     return FD2_OK;
 }
 
@@ -63,10 +93,14 @@ int fd2_context_create(int device, fd2_context** out) {
 int fd2_context_destroy(fd2_context* c) {
     if (!c) return FD2_OK;
     cudaSetDevice(c->device);
+    cudaDeviceSynchronize();  // no work of any stream still uses the context's memory
     for (void* b : c->buf)
-        if (b) cudaFree(b);
+        if (b) cudaFreeAsync(b, c->stream);
     if (c->d_status) cudaFree(c->d_status);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
     if (c->pool) {
         cudaDeviceSynchronize();  // stream-ordered frees on other streams complete first
         cudaMemPoolDestroy(c->pool);
@@ -139,7 +173,12 @@ int fd2_density_create(fd2_context* ctx, const float* host_density, const fd2_vo
 
 int fd2_density_destroy(fd2_density* d) {
     if (!d) return FD2_OK;
-    if (d->d_density) cudaFree(d->d_density);
+    if (d->d_density) {
+        if (d->pooled)
+            cudaFreeAsync(d->d_density, d->ctx->stream);
+        else
+            cudaFree(d->d_density);
+    }
     delete d;
     return FD2_OK;
 }

@@ -266,7 +266,7 @@ static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const 
         FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz_bound + cap[nb]));
         const uint64_t ncap = std::max<uint64_t>(1, cap[nb]);
         void* tmp = nullptr;
-        FD2_TRY(ctx_buffer(ctx, kBufColumns, ncap * (sizeof(int32_t) + sizeof(float)), &tmp));
+        FD2_TRY(ctx_buffer(ctx, kBufColumns, ncap * (sizeof(int32_t) + sizeof(float)), st, &tmp));
         int32_t* d_tcol = (int32_t*)tmp;
         float* d_tval = (float*)(d_tcol + ncap);
         FD2_TRY(upload(cap, &d_cap_off, ctx->pool, st));
@@ -434,6 +434,8 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     if (params_in) params = *params_in;
     FD2_REQUIRE(params.ss_factor > 0 && params.ss_factor <= 16, FD2_ERR_INVALID_ARGUMENT, "ss_factor out of range");
     FD2_REQUIRE(params.value_type >= 0 && params.value_type <= 2, FD2_ERR_INVALID_ARGUMENT, "bad value type");
+    FD2_REQUIRE(params.cccs_schedule >= -2 && params.cccs_schedule <= 1, FD2_ERR_INVALID_ARGUMENT,
+                "cccs_schedule %d (-2..1)", params.cccs_schedule);
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const fd2_volume_t& vol = density->vol;
     const uint64_t nvox = (uint64_t)vol.dim[0] * vol.dim[1] * vol.dim[2];
@@ -519,7 +521,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         std::vector<size_t> off(nb + 1, 0);
         for (size_t k = 0; k < nb; k++) off[k + 1] = off[k] + (size_t)beams[b0 + k].long_dim * P;
         float* d_bev = nullptr;
-        rc = ctx_buffer(ctx, kBufBev, off[nb] * 3 * sizeof(float), (void**)&d_bev);
+        rc = ctx_buffer(ctx, kBufBev, off[nb] * 3 * sizeof(float), st, (void**)&d_bev);
         if (rc) break;
         float *dT = d_bev, *dR = d_bev + off[nb], *dD = d_bev + 2 * off[nb];
         std::vector<const float*> hF(nb, d_fluence);
@@ -546,6 +548,8 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
                 };
                 if (params.cccs_schedule >= 0) {
                     FD2_TRY(run(params.cccs_schedule));
+                } else if (params.cccs_schedule == -2) {
+                    FD2_TRY(run(cccs_auto_schedule(ctx, nb)));
                 } else {
                     FD2_TRY(tuned_cccs(ctx, nb, P, kernel, st, run, dD, off[nb]));
                 }

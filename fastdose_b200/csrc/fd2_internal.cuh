@@ -64,6 +64,7 @@ struct fd2_context {
     // reusable grow-only device buffers (fd2::ctx_buffer slots), kept between calls
     void* buf[4] = {nullptr, nullptr, nullptr, nullptr};
     size_t buf_bytes[4] = {0, 0, 0, 0};
+    cudaStream_t buf_stream[4] = {nullptr, nullptr, nullptr, nullptr};  // stream of each buffer's last use
     // stream-ordered pool for batch buffers and dose-matrix storage; it keeps
     // freed memory (release threshold = max) so repeated plans reuse it
     cudaMemPool_t pool = nullptr;
@@ -110,6 +111,7 @@ struct fd2_density {
     fd2_context* ctx = nullptr;
     fd2_volume_t vol{};
     float* d_density = nullptr;  // float[z][y][x]
+    bool pooled = false;         // from the context's pool in its stream's order (density_create_pooled)
 };
 
 struct fd2_spectrum {
@@ -130,13 +132,23 @@ struct fd2_cccs_kernel {
 
 namespace fd2 {
 
-// Grow-only device buffers owned by a context, one per use.  A buffer is
-// reused by every later call on the context (calls on one context are
-// serialised: one host thread, work in stream order); growing it frees the old
-// one, which waits for the device.
+// Grow-only device buffers owned by a context, one per use, from the
+// context's pool.  A buffer is reused by every later call on the context
+// (calls on one context are serialised: one host thread, work in stream
+// order); growing it replaces the old one in the order of stream `st`, and
+// waits for the device only when the previous use was on another stream.
 enum CtxBuffer { kBufCccs = 0, kBufBev = 1, kBufColumns = 2, kBufCount = 4 };
-int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, void** out);
-inline int ctx_scratch(fd2_context* ctx, size_t bytes, void** out) { return ctx_buffer(ctx, kBufCccs, bytes, out); }
+int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, cudaStream_t st, void** out);
+inline int ctx_scratch(fd2_context* ctx, size_t bytes, cudaStream_t st, void** out) {
+    return ctx_buffer(ctx, kBufCccs, bytes, st, out);
+}
+
+// A density whose device copy comes from the context's pool in the order of
+// the context's stream, and returns to it the same way on destroy: no call
+// that waits for the whole device.  Only for work issued on ctx->stream (a
+// service worker's requests); the public fd2_density_create allocates plainly.
+int density_create_pooled(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume,
+                          fd2_density** out);
 
 // Spectrum table passed by value to kernels (lives in the kernel parameter
 // space, not in process-global __constant__ memory).

@@ -90,7 +90,10 @@ int run_request(fd2_context* ctx, Request& r) {
     fd2_density* d = nullptr;
     fd2_spectrum* sp = nullptr;
     fd2_cccs_kernel* k = nullptr;
-    int rc = fd2_density_create(ctx, r.density.data(), &r.vol, &d);
+    // every allocation of a request is stream-ordered on the worker's stream:
+    // a free that waited for the whole device would wait for the other
+    // workers' requests too
+    int rc = fd2::density_create_pooled(ctx, r.density.data(), &r.vol, &d);
     if (!rc)
         rc = fd2_spectrum_create(ctx, (int)r.energy.size(), r.energy.data(), r.sfl.data(), r.mu.data(),
                                  r.mu_en.data(), &sp);
@@ -227,6 +230,9 @@ int fd2_service_submit(fd2_service* s, const fd2_plan_request_t* q, uint64_t* ti
     r->params = q->params;
     r->params.memory_budget = s->bev_budget;
     r->params.host_out = nullptr;  // a served request's result stays on the device
+    // a request's latency must not carry a timing run of both CCCS schedules
+    // (each new batch shape would add one): served requests take the rule
+    if (r->params.cccs_schedule == -1) r->params.cccs_schedule = -2;
     r->stats.beamlets = total;
     r->stats.est_bytes = estimate_bytes(*r, s->bev_budget);
     FD2_REQUIRE(r->stats.est_bytes <= s->budget, FD2_ERR_ADMISSION,

@@ -59,7 +59,9 @@ typedef struct fd2_dosemat_params {
     float extent;               /* cm; voxels farther from a beamlet axis are 0 (default 2.0) */
     int ss_factor;              /* supersampling per axis of the column stage (default 5) */
     int value_type;             /* fd2_value_type (default F32) */
-    int cccs_schedule;          /* -1 auto, 0 zenith loop per block, 1 zenith split */
+    int cccs_schedule;          /* -1 auto (both timed on the first batch of a shape, the faster kept),
+                                   -2 rule (zenith split below 4 blocks per SM; no timing run),
+                                   0 zenith loop per block, 1 zenith split */
     uint64_t batch_beamlets;    /* 0 = auto (memory budget) */
     uint64_t memory_budget;     /* bytes of BEV scratch per batch; 0 = auto */
     int verbose;                /* print per-batch timings to stdout */
