@@ -117,6 +117,17 @@ int run_request(fd2_context* ctx, Request& r) {
 void worker_main(fd2_service* s, int index) {
     fd2_context* ctx = nullptr;
     const int crc = fd2_context_create(s->device, &ctx);
+    if (!crc) {
+        // Grow the worker's pool once, up front, by a request's usual working
+        // set (one batch of BEV volumes and as much again for the matrix and
+        // the column scratch): mapping new device memory while the other
+        // workers' kernels run stalls them, so requests should find it mapped.
+        void* p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, 2 * s->bev_budget, ctx->pool, ctx->stream) == cudaSuccess)
+            cudaFreeAsync(p, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
+        cudaGetLastError();  // an oversized reserve is not an error of the service
+    }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->contexts[index] = ctx;
