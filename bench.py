@@ -713,7 +713,7 @@ def run_fd2(args, rank, world):
     L = np.concatenate([b["long_dim"] for b in beamlets]).astype(np.float64)
     cccs_bytes = float(np.sum(4.0 * P * L * 3))  # Terma + density read, dose written, per beamlet
     # DRAM bytes the CCCS kernel moves per beamlet: dram__bytes_read.sum + dram__bytes_write.sum of one
-    # ncu capture on the 4-beam plan (610 beamlets, 3.80 GB; profiles/cccs_kernel_4pi_torso_4beams.md),
+    # ncu capture of the march on the 4-beam plan (610 beamlets, 3.80 GB),
     # scaled by the beamlets of this step (each zenith pass re-reads its slices: traffic grows with beamlets)
     cccs_traffic = CCCS_DRAM_BYTES_PER_BEAMLET * n_bl
     cccs_ms = stages["cccs"]
