@@ -310,7 +310,7 @@ struct HostSink {
     bool have_pending = false;
     Batch pending;
 
-    int init(fd2_host_csr_t* o, fd2_csr_ensemble* ens, uint64_t n_rows) {
+    int init(fd2_host_csr_t* o, fd2_csr_ensemble* ens) {
         FD2_REQUIRE(o->row_off && o->col && o->val, FD2_ERR_INVALID_ARGUMENT,
                     "dose_mat_construct: host_out needs row_off, col and val");
         FD2_REQUIRE(ens->value_type == FD2_VALUES_F32 || o->scale, FD2_ERR_INVALID_ARGUMENT,
@@ -319,7 +319,6 @@ struct HostSink {
         e = ens;
         out->nnz = 0;
         out->row_off[0] = 0;
-        (void)n_rows;
         FD2_CHECK_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
         return FD2_OK;
     }
@@ -476,7 +475,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     for (uint32_t c : cnt) cap_total += c;
     if (!rc) rc = ensemble_reserve(e, total, cap_total);
     HostSink sink;  // declared before the ensemble is destroyed on any path: its copies finish first
-    if (!rc && params.host_out) rc = sink.init(params.host_out, e, total);
+    if (!rc && params.host_out) rc = sink.init(params.host_out, e);
     if (rc) {
         if (d_infos) cudaFreeAsync(d_infos, st);
         fd2_csr_ensemble_destroy(e);

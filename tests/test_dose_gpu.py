@@ -88,6 +88,24 @@ def _dense(ro, col, val, n_rows, n_cols):
     return out
 
 
+def test_rule_cccs_schedule(ctx):
+    """cccs_schedule = -2 picks a schedule by rule, without a timing run: the
+    same matrix as either fixed schedule, bit for bit, and nothing tuned."""
+    from fastdose_b200 import _lib
+
+    c2 = api.Context(0)
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(c2, case)
+    ref = api.DoseMatConstruction(c2, [case["beams"]], case["fluence"], dens, sp, kn, cccs_schedule=0).to_host()
+    rule = api.DoseMatConstruction(c2, [case["beams"]], case["fluence"], dens, sp, kn, cccs_schedule=-2)
+    for a, b in zip(rule.to_host(), ref):
+        np.testing.assert_array_equal(a, b)
+    assert c2.tuned_schedules() == ({}, 0)
+    with pytest.raises(_lib.FD2Error):
+        api.DoseMatConstruction(c2, [case["beams"]], case["fluence"], dens, sp, kn, cccs_schedule=-3)
+    rule.close()
+
+
 def test_tuned_cccs_schedule(ctx):
     """The automatic schedule times both schedules on the first batch of a
     shape, then reuses the choice; every build gives the same matrix as either
@@ -235,7 +253,7 @@ def _decode16(words, scale, ro, vt):
     return (v * np.asarray(scale, np.float32)[rows]).astype(np.float32)
 
 
-@pytest.mark.parametrize("vt", ["f32", "f16"])
+@pytest.mark.parametrize("vt", ["f32", "f16", "bf16"])
 def test_host_copy_while_building(ctx, vt):
     """host_out receives the matrix batch by batch during the construction
     (small batches force several overlapped copies): the same arrays as the
