@@ -176,8 +176,9 @@ __device__ __forceinline__ float seg_length(float l2) {
 // so the x half of the voxel work is done once per lane and the y half once per
 // row and shared by shuffles (16 x 16 maps share it through the row table);
 // RPL >= ceil(F / k).
-template <int RPL, bool kFx16, bool kCols = false>
-__global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 4 : ((kCols && RPL <= 8) ? 4 : (kCols ? 3 : 1)))
+template <int RPL, bool kFx16, bool kCols = false, bool kTab = false>
+__global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
+                                  kFx16 ? 4 : ((kCols || kTab) && RPL <= 8 ? 4 : (kCols || kTab ? 3 : 1)))
     cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
@@ -210,6 +211,16 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 4
     g.lim_min = b.lim_min;
     g.inv_sad = 1.0f / b.sad;
     const size_t pitch = b.TermaBEV_pitch / sizeof(float);
+
+    // kTab: per block, the (column, row) table entries of ray j of each lane
+    // (x entry = column, y entry = F + row; all ones past the map), and per
+    // azimuth warp the step's 2F halves
+    __shared__ uint32_t s_pairs[kTab ? RPL * 32 : 1];
+    __shared__ float2 s_htab[kTab ? 8 * 64 : 1];
+    if constexpr (kTab) {
+        for (int i = threadIdx.x; i < RPL * 32; i += blockDim.x)  // ray i / 32 of lane i % 32 is cell i
+            s_pairs[i] = i < g.P ? (uint32_t)(i % g.fx) | (uint32_t)(g.fx + i / g.fx) << 16 : 0xffffffffu;
+    }  // visible after the first slice's barrier
 
     float2* tr = smem;
     float2* dp = smem + g.P;
@@ -385,6 +396,51 @@ __global__ void __launch_bounds__(kFx16 || kCols ? kFx16Threads : 768, kFx16 ? 4
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
                     }
+                } else if constexpr (kTab) {
+                    // F x F map, F <= 24: the rays of lane l are the cells l + 32 j,
+                    // so all 32 lanes carry rays whatever F.  The step's 2F halves
+                    // (x of each column, y of each row) are evaluated once, one per
+                    // lane and round, into the warp's half table {+-|offset|,
+                    // bytes into the slice}, the edge crossing as the sign bit;
+                    // each ray then reads its column's and its row's entry.
+                    float2* ht = s_htab + 64 * warp;
+                    for (int h = lane; h < 2 * g.fx; h += 32) {
+                        const bool yh = h >= g.fx;
+                        const float off = (float)(yh ? h - g.fx : h);
+                        const float hb = __fadd_rn(yh ? c.y : c.x, off), hn = __fadd_rn(yh ? np.y : np.x, off);
+                        const float ff = yh ? g.ffy : g.ffx, hh = yh ? g.hy : g.hx, bs = yh ? g.bsy : g.bsx;
+                        const int hi = mid_index(hb, hn, ff, yh ? g.fy : g.fx);
+                        const float hq = fabsf((hn - hh) * bs * fe - (hb - hh) * bs * fs);
+                        const float hs = crosses_edge(hb, hn, ff) ? -hq : hq;
+                        const int bytes = (int)sizeof(float2) * (yh ? hi * g.fx : hi);
+                        ht[h] = make_float2(hs, __int_as_float(bytes));
+                    }
+                    __syncwarp();
+                    const float dz2 = dzp * dzp;
+#pragma unroll
+                    for (int j = 0; j < RPL; j++) {
+                        const uint32_t pr = s_pairs[32 * j + lane];
+                        const bool on = pr != 0xffffffffu;
+                        const float2 xe = ht[on ? (pr & 0xffffu) : 0], ye = ht[on ? (pr >> 16) : 0];
+                        const bool wrap = (__float_as_int(xe.x) | __float_as_int(ye.x)) < 0;
+                        const int mb = __float_as_int(xe.y) + __float_as_int(ye.y);
+                        const float dxz2 = xe.x * xe.x + dz2;
+                        const float l2 = dxz2 + ye.x * ye.x;
+                        const float len = seg_length(l2);
+                        const float2 trv = *reinterpret_cast<const float2*>(reinterpret_cast<const char*>(tr) + mb);
+                        const float p = len * trv.y;
+                        const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
+                        const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
+                        if (on) {
+                            float2* acc_p = reinterpret_cast<float2*>(reinterpret_cast<char*>(mydp) + mb);
+                            float2 acc = *acc_p;
+                            acc.x += dep;
+                            acc.y += p;
+                            *acc_p = acc;
+                        }
+                        XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
+                        XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
+                    }
                 } else {
 #pragma unroll
                 for (int j = 0; j < RPL; j++) {
@@ -474,13 +530,13 @@ __global__ void cccs_split_reduce(const fd2_beam_t* __restrict__ beams, float* c
     }
 }
 
-template <int RPL, bool kFx16, bool kCols>
+template <int RPL, bool kFx16, bool kCols, bool kTab = false>
 int launch_instance(unsigned blocks, int threads, size_t shm, cudaStream_t st, const fd2_beam_t* d_beams,
                     const float* const* T, const float* const* R, float* const* D, const float4* dirs,
                     const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status) {
-    FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<RPL, kFx16, kCols>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<RPL, kFx16, kCols, kTab>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)shm));
-    cccs_kernel<RPL, kFx16, kCols><<<blocks, threads, shm, st>>>(d_beams, T, R, D, dirs, cp, split, planes,
+    cccs_kernel<RPL, kFx16, kCols, kTab><<<blocks, threads, shm, st>>>(d_beams, T, R, D, dirs, cp, split, planes,
                                                                  plane_stride, status);
     FD2_CHECK_CUDA(cudaGetLastError());
     return FD2_OK;
@@ -499,6 +555,23 @@ int launch_march(int map, int maxP, int n_phi, unsigned blocks, cudaStream_t st,
     if (map == 16 && threads <= kFx16Threads)
         return launch_instance<8, true, false>(blocks, threads, (size_t)n_phi * (256 * sizeof(float4) + 16 * sizeof(float2)),
                                                st, d_beams, T, R, D, dirs, cp, split, planes, plane_stride, status);
+    if (map > 0 && map <= 24 && warps_ok) {  // half-table instance: rays per lane = ceil(F^2 / 32)
+        const int P = map * map;
+        if (P <= 64)
+            return launch_instance<2, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                          planes, plane_stride, status);
+        if (P <= 160)
+            return launch_instance<5, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                          planes, plane_stride, status);
+        if (P <= 256)
+            return launch_instance<8, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                          planes, plane_stride, status);
+        if (P <= 416)
+            return launch_instance<13, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp,
+                                                           split, planes, plane_stride, status);
+        return launch_instance<18, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
+                                                       planes, plane_stride, status);
+    }
     if (map > 0 && map <= 32 && warps_ok) {
         const int k = 32 / map, rows = (map + k - 1) / k;  // rows per lane
         if (rows <= 8)
