@@ -149,6 +149,16 @@ __device__ __forceinline__ bool crosses16(float b, float n) {
     return floorf(__fmul_rn(b, 0.0625f)) != floorf(__fmul_rn(n, 0.0625f));
 }
 
+// 4 bytes from global to shared memory without passing through registers
+// (PTX cp.async), committed as one group per call site; and the wait for all
+// of this thread's groups.
+__device__ __forceinline__ void cp_async4(float* smem_dst, const float* gsrc) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // 2^x on the special-function unit (PTX ex2.approx.ftz.f32).  The attenuation
 // e^(-k p) is evaluated as 2^(-(k log2 e) p) with k log2 e formed once per
 // zenith bin: one multiply and one MUFU operation per exponential.
@@ -256,9 +266,14 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
     const float fcol = (float)ccol, frow = (float)(kCols && lane < g.fy ? lane : 0);
 
     // register prefetch of the next slice's Terma/density (one pixel per thread)
-    const bool prefetch = g.P <= (int)blockDim.x;
+    const bool prefetch = !kFx16 && g.P <= (int)blockDim.x;
     int pf_s = -1;
     float2 pf = make_float2(0.0f, 0.0f);
+    // kFx16: the slice most likely to come next, copied by cp.async into
+    // s_stage (Terma, then density) during the march; each thread copies and
+    // later reads the same pixels, so no barrier stands between the two
+    __shared__ float s_stage[kFx16 ? 2 * 256 : 1];
+    int st_s = -1;
 
     for (int t = t0; t < t1; t++) {
         const float Aa = cp.A_a[t], Bb = cp.B_b[t];
@@ -282,8 +297,9 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
         while (s < g.L) {
             if constexpr (kFx16) {
                 // each pixel's pair goes to every azimuth's copy, sums cleared
+                cp_async_wait_all();  // this thread's staged pixels have landed
                 for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
-                    const float2 t = s == pf_s ? pf
+                    const float2 t = s == st_s ? make_float2(s_stage[v], s_stage[256 + v])
                                                : make_float2(__ldg(T + (size_t)s * pitch + v),
                                                              __ldg(R + (size_t)s * pitch + v));
                     for (int w = 0; w < n_phi; w++) wb[(size_t)w * g.P + v] = make_float4(t.x, t.y, 0.0f, 0.0f);
@@ -301,6 +317,15 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
             // Prefetch the slice most likely to come next (s + 1, or slice 0 of
             // the next zenith bin) into registers; its loads are in flight during
             // the march and are used only if that slice is the one taken.
+            if constexpr (kFx16) {
+                st_s = s + 1 < g.L ? s + 1 : (t + 1 < t1 ? 0 : -1);
+                if (st_s >= 0)
+                    for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
+                        cp_async4(&s_stage[v], T + (size_t)st_s * pitch + v);
+                        cp_async4(&s_stage[256 + v], R + (size_t)st_s * pitch + v);
+                    }
+                cp_async_commit();
+            }
             pf_s = -1;
             if (prefetch) {
                 pf_s = s + 1 < g.L ? s + 1 : (t + 1 < t1 ? 0 : -1);
@@ -511,6 +536,7 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
             s = s_new;
         }
     }
+    if constexpr (kFx16) cp_async_wait_all();  // a staged slice that was not taken
 }
 
 // dose_bev[s][v] += sum_t planes[t][s][v] (zenith bins in order)
