@@ -35,7 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "CCCS beamlets/s (dose-loading matrix, batched 4pi)"
-CCCS_DRAM_BYTES_PER_BEAMLET = 3.7978e9 / 610
+CCCS_DRAM_BYTES_PER_BEAMLET = 3.7754e9 / 610
 UNIT = "beamlets/s"
 
 
@@ -714,7 +714,7 @@ def run_fd2(args, rank, world):
     L = np.concatenate([b["long_dim"] for b in beamlets]).astype(np.float64)
     cccs_bytes = float(np.sum(4.0 * P * L * 3))  # Terma + density read, dose written, per beamlet
     # DRAM bytes the CCCS kernel moves per beamlet: dram__bytes_read.sum + dram__bytes_write.sum of one
-    # ncu capture of the march on the 4-beam plan (610 beamlets, 3.80 GB),
+    # ncu capture of the march on the 4-beam plan (610 beamlets, 3.78 GB),
     # scaled by the beamlets of this step (each zenith pass re-reads its slices: traffic grows with beamlets)
     cccs_traffic = CCCS_DRAM_BYTES_PER_BEAMLET * n_bl
     cccs_ms = stages["cccs"]
