@@ -139,6 +139,12 @@ def cpu_baseline(cfg, beamlets, fluence, budget_s, threads):
             "sample": f"{done} of {len(flat)} beamlets of the same plan (Terma, CCCS, column), {dt:.1f} s"}
 
 
+def workload_name(n_beams, n_beamlets):
+    """The bench workload, named the same by both arms."""
+    return (f"4pi torso 200x200x160 @2.5mm, {n_beams} beams, {n_beamlets} beamlets (16x16, 0.5 cm), "
+            f"8x6 cones, 12-bin spectrum")
+
+
 def run_reference(args, rank):
     """--impl reference: the reference has no CPU implementation of this path;
     its algorithm is timed through the CPU restatement on all host cores."""
@@ -161,6 +167,7 @@ def run_reference(args, rank):
         beams0 = np.array([api.calc_range(_bundle_beam(b), ph.volume) for b in bundles])
         flags = oracle.beamlet_flags(beams0, ph.masks["PTV"], ph.volume, tex_mode=1)
     beamlets = api.bundles_beamlets(bundles, flags, ph.volume)
+    n_bl = int(sum(len(b) for b in beamlets))
     fluence = api.beamlet_fluence(bundles[0])
     threads = os.cpu_count() or 1
     steps = []
@@ -172,7 +179,8 @@ def run_reference(args, rank):
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": {"workload": "4pi torso 200x200x160 @2.5mm, %d beams x 16x16 beamlets, 8x6 cones" % len(bundles)},
+            "config": {"workload": workload_name(len(bundles), n_bl), "beams": len(bundles), "beamlets": n_bl,
+                       "parallelism": f"CPU restatement on {threads} host threads"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": r["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -743,8 +751,7 @@ def run_fd2(args, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"4pi torso 200x200x160 @2.5mm, {len(bundles)} beams, {n_bl_total} beamlets (16x16, 0.5 cm), "
-                               f"8x6 cones, 12-bin spectrum", "beams": len(bundles), "beamlets": n_bl_total,
+        "config": {"workload": workload_name(len(bundles), n_bl_total), "beams": len(bundles), "beamlets": n_bl_total,
                    "beams_per_rank": [len(p) for p in parts],
                    "nnz": int(info["nnz"]), "l2": "inputs and BEV scratch larger than L2 (126 MB)",
                    "parallelism": f"beams partitioned over {world} GPU(s), no collective"},
