@@ -265,14 +265,12 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
     const bool clane = kCols && lane < kgrp * g.fx;
     const float fcol = (float)ccol, frow = (float)(kCols && lane < g.fy ? lane : 0);
 
-    // register prefetch of the next slice's Terma/density (one pixel per thread)
-    const bool prefetch = !kFx16 && g.P <= (int)blockDim.x;
-    int pf_s = -1;
-    float2 pf = make_float2(0.0f, 0.0f);
-    // kFx16: the slice most likely to come next, copied by cp.async into
-    // s_stage (Terma, then density) during the march; each thread copies and
-    // later reads the same pixels, so no barrier stands between the two
-    __shared__ float s_stage[kFx16 ? 2 * 256 : 1];
+    // The slice most likely to come next (s + 1, or slice 0 of the next zenith
+    // pass), copied by cp.async into s_stage (Terma, then density) during the
+    // march and used only if that slice is the one taken.  Each thread copies
+    // and later reads the same pixels, so no barrier stands between the two.
+    constexpr int kStageP = kFx16 ? 256 : 1024;
+    __shared__ float s_stage[2 * kStageP];
     int st_s = -1;
 
     for (int t = t0; t < t1; t++) {
@@ -299,40 +297,26 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                 // each pixel's pair goes to every azimuth's copy, sums cleared
                 cp_async_wait_all();  // this thread's staged pixels have landed
                 for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
-                    const float2 t = s == st_s ? make_float2(s_stage[v], s_stage[256 + v])
+                    const float2 t = s == st_s ? make_float2(s_stage[v], s_stage[kStageP + v])
                                                : make_float2(__ldg(T + (size_t)s * pitch + v),
                                                              __ldg(R + (size_t)s * pitch + v));
                     for (int w = 0; w < n_phi; w++) wb[(size_t)w * g.P + v] = make_float4(t.x, t.y, 0.0f, 0.0f);
                 }
             } else {
-                if (s == pf_s) {
-                    if (threadIdx.x < g.P) tr[threadIdx.x] = pf;
-                } else {
-                    for (int v = threadIdx.x; v < g.P; v += blockDim.x)
-                        tr[v] = make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
-                }
+                cp_async_wait_all();  // this thread's staged pixels have landed
+                for (int v = threadIdx.x; v < g.P; v += blockDim.x)
+                    tr[v] = s == st_s ? make_float2(s_stage[v], s_stage[kStageP + v])
+                                      : make_float2(__ldg(T + (size_t)s * pitch + v), __ldg(R + (size_t)s * pitch + v));
                 for (int v = lane; v < g.P; v += 32) mydp[v] = make_float2(0.0f, 0.0f);
             }
             __syncthreads();
-            // Prefetch the slice most likely to come next (s + 1, or slice 0 of
-            // the next zenith bin) into registers; its loads are in flight during
-            // the march and are used only if that slice is the one taken.
-            if constexpr (kFx16) {
-                st_s = s + 1 < g.L ? s + 1 : (t + 1 < t1 ? 0 : -1);
-                if (st_s >= 0)
-                    for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
-                        cp_async4(&s_stage[v], T + (size_t)st_s * pitch + v);
-                        cp_async4(&s_stage[256 + v], R + (size_t)st_s * pitch + v);
-                    }
-                cp_async_commit();
-            }
-            pf_s = -1;
-            if (prefetch) {
-                pf_s = s + 1 < g.L ? s + 1 : (t + 1 < t1 ? 0 : -1);
-                if (pf_s >= 0 && threadIdx.x < g.P)
-                    pf = make_float2(__ldg(T + (size_t)pf_s * pitch + threadIdx.x),
-                                     __ldg(R + (size_t)pf_s * pitch + threadIdx.x));
-            }
+            st_s = s + 1 < g.L ? s + 1 : (t + 1 < t1 ? 0 : -1);
+            if (st_s >= 0)
+                for (int v = threadIdx.x; v < g.P; v += blockDim.x) {
+                    cp_async4(&s_stage[v], T + (size_t)st_s * pitch + v);
+                    cp_async4(&s_stage[kStageP + v], R + (size_t)st_s * pitch + v);
+                }
+            cp_async_commit();
 
             int guard = 0;
             for (;;) {
@@ -536,7 +520,7 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
             s = s_new;
         }
     }
-    if constexpr (kFx16) cp_async_wait_all();  // a staged slice that was not taken
+    cp_async_wait_all();  // a staged slice that was not taken
 }
 
 // dose_bev[s][v] += sum_t planes[t][s][v] (zenith bins in order)
