@@ -781,6 +781,13 @@ def run_fd2(args, rank, world):
         sb["batched_speedup"] = value / world / sb["value"]
         line["single_beam"] = sb
         line["optimizer"] = optimizer_leg(ctx, args.opt_iters, args.opt_rows)
+        # the service's worker contexts start from a device the earlier legs
+        # have handed back, as a service process would find it
+        import gc
+
+        gc.collect()
+        torch.cuda.empty_cache()
+        ctx.release()
         line["served"] = served_leg(ctx)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, os.cpu_count() or 1)

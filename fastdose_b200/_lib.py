@@ -27,6 +27,7 @@ _PROTOS = {
     "fd2_context_create": (_i, [_i, _vp]),
     "fd2_context_destroy": (_i, [_vp]),
     "fd2_context_synchronize": (_i, [_vp]),
+    "fd2_context_release": (_i, [_vp]),
     "fd2_density_create": (_i, [_vp, _vp, _vp, _vp]),
     "fd2_density_destroy": (_i, [_vp]),
     "fd2_density_device_ptr": (_vp, [_vp]),

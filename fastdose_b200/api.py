@@ -98,6 +98,10 @@ class Context:
     def synchronize(self):
         _lib.check(self.lib.fd2_context_synchronize(self.h), "context_synchronize")
 
+    def release(self):
+        """Return the context's idle device memory (fd2_context_release)."""
+        _lib.check(self.lib.fd2_context_release(self.h), "context_release")
+
     STAGES = ("terma", "cccs", "columns", "opt_spmv", "opt_other")
 
     def tuned_schedules(self):

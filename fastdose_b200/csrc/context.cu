@@ -109,6 +109,20 @@ int fd2_context_destroy(fd2_context* c) {
     return FD2_OK;
 }
 
+int fd2_context_release(fd2_context* c) {
+    FD2_REQUIRE(c, FD2_ERR_INVALID_ARGUMENT, "null context");
+    FD2_CHECK_CUDA(cudaDeviceSynchronize());  // no work of any stream still uses the buffers
+    for (int i = 0; i < fd2::kBufCount; i++) {
+        if (c->buf[i]) FD2_CHECK_CUDA(cudaFreeAsync(c->buf[i], c->stream));
+        c->buf[i] = nullptr;
+        c->buf_bytes[i] = 0;
+        c->buf_stream[i] = nullptr;
+    }
+    FD2_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    FD2_CHECK_CUDA(cudaMemPoolTrimTo(c->pool, 0));
+    return FD2_OK;
+}
+
 int fd2_context_synchronize(fd2_context* c) {
     FD2_REQUIRE(c, FD2_ERR_INVALID_ARGUMENT, "null context");
     FD2_CHECK_CUDA(cudaStreamSynchronize(c->stream));

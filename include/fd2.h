@@ -140,6 +140,15 @@ int fd2_context_create(int device, fd2_context** out);
 int fd2_context_destroy(fd2_context* ctx);
 /* Synchronises the context's internal streams. */
 int fd2_context_synchronize(fd2_context* ctx);
+/*
+ * Returns the context's idle device memory: waits for the device, frees the
+ * grow-only BEV, column and cone buffers, and trims the context's pool to the
+ * allocations still alive (matrices not yet destroyed keep theirs).  The next
+ * call regrows what it needs.  For a process that moves from one workload to
+ * another on the same GPU (e.g. from building matrices to serving requests on
+ * other contexts).
+ */
+int fd2_context_release(fd2_context* ctx);
 
 /*
  * Instrumentation, the counterpart of the reference's per-kernel event timers
