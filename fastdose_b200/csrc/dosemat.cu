@@ -790,6 +790,85 @@ static int read_file(const std::string& path, std::vector<char>& out) {
     return FD2_OK;
 }
 
+// 64-bit voxel indices of a doseMatFolder to the ensemble's int32 columns;
+// an index outside the volume sets *bad.
+__global__ void columns_from_file_kernel(const uint64_t* __restrict__ in, int32_t* __restrict__ out, size_t n,
+                                         uint64_t n_cols, unsigned int* __restrict__ bad) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const uint64_t c = in[i];
+        if (c >= n_cols) {
+            atomicOr(bad, 1u);
+            out[i] = 0;
+        } else {
+            out[i] = (int32_t)c;
+        }
+    }
+}
+
+// columnsBuffer.bin and the values file streamed to the device in chunks:
+// while the device converts and stores chunk i (from a pinned buffer), the
+// host reads chunk i + 1 into the other one.  Host memory stays at two chunks,
+// whatever the matrix.
+static int stream_columns(fd2_context* ctx, const std::string& col_path, const std::string& val_path, uint64_t nnz,
+                          size_t vb, uint64_t n_cols, int32_t* d_col, void* d_val, cudaStream_t st) {
+    constexpr size_t kChunk = (size_t)4 << 20;  // nonzeros per chunk: 32 MB of 64-bit columns
+    struct Res {
+        FILE* fc = nullptr;
+        FILE* fv = nullptr;
+        void* h[4] = {nullptr, nullptr, nullptr, nullptr};  // columns 0/1, values 0/1 (pinned)
+        void* d_c64[2] = {nullptr, nullptr};
+        unsigned int* d_bad = nullptr;
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        cudaStream_t st = nullptr;
+        ~Res() {
+            if (st) cudaStreamSynchronize(st);  // no copy still reads the pinned buffers
+            if (fc) fclose(fc);
+            if (fv) fclose(fv);
+            for (void* p : h)
+                if (p) cudaFreeHost(p);
+            for (void* p : d_c64)
+                if (p) cudaFreeAsync(p, st);
+            if (d_bad) cudaFreeAsync(d_bad, st);
+            for (cudaEvent_t e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } res;
+    if (nnz == 0) return FD2_OK;
+    res.st = st;
+    res.fc = fopen(col_path.c_str(), "rb");
+    res.fv = fopen(val_path.c_str(), "rb");
+    FD2_REQUIRE(res.fc && res.fv, FD2_ERR_IO, "fromfile: cannot open %s or %s", col_path.c_str(), val_path.c_str());
+    const size_t chunk = std::min<size_t>(kChunk, nnz);
+    for (int b = 0; b < 2; b++) {
+        FD2_CHECK_CUDA(cudaHostAlloc(&res.h[b], chunk * 8, cudaHostAllocDefault));
+        FD2_CHECK_CUDA(cudaHostAlloc(&res.h[2 + b], chunk * vb, cudaHostAllocDefault));
+        FD2_CHECK_CUDA(cudaMallocFromPoolAsync(&res.d_c64[b], chunk * 8, ctx->pool, st));
+        FD2_CHECK_CUDA(cudaEventCreateWithFlags(&res.ev[b], cudaEventDisableTiming));
+    }
+    FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&res.d_bad, sizeof(unsigned int), ctx->pool, st));
+    FD2_CHECK_CUDA(cudaMemsetAsync(res.d_bad, 0, sizeof(unsigned int), st));
+    for (uint64_t k0 = 0, i = 0; k0 < nnz; k0 += chunk, i++) {
+        const int b = (int)(i & 1);
+        const size_t n = (size_t)std::min<uint64_t>(chunk, nnz - k0);
+        if (i >= 2) FD2_CHECK_CUDA(cudaEventSynchronize(res.ev[b]));  // buffer b's last copies are done
+        FD2_REQUIRE(fread(res.h[b], 8, n, res.fc) == n && fread(res.h[2 + b], vb, n, res.fv) == n, FD2_ERR_IO,
+                    "fromfile: short read at nonzero %llu", (unsigned long long)k0);
+        FD2_CHECK_CUDA(cudaMemcpyAsync(res.d_c64[b], res.h[b], n * 8, cudaMemcpyHostToDevice, st));
+        const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->sm_count * 8);
+        columns_from_file_kernel<<<blocks, 256, 0, st>>>((const uint64_t*)res.d_c64[b], d_col + k0, n, n_cols,
+                                                         res.d_bad);
+        FD2_CHECK_CUDA(cudaGetLastError());
+        FD2_CHECK_CUDA(cudaMemcpyAsync((char*)d_val + k0 * vb, res.h[2 + b], n * vb, cudaMemcpyHostToDevice, st));
+        FD2_CHECK_CUDA(cudaEventRecord(res.ev[b], st));
+    }
+    unsigned int bad = 0;
+    FD2_CHECK_CUDA(cudaMemcpyAsync(&bad, res.d_bad, sizeof(bad), cudaMemcpyDeviceToHost, st));
+    FD2_CHECK_CUDA(cudaStreamSynchronize(st));
+    FD2_REQUIRE(!bad, FD2_ERR_IO, "fromfile: a column index is outside the %llu-voxel volume",
+                (unsigned long long)n_cols);
+    return FD2_OK;
+}
+
 int fd2_csr_ensemble_tofile(const fd2_csr_ensemble* e, const char* folder) {
     FD2_REQUIRE(e && folder, FD2_ERR_INVALID_ARGUMENT, "tofile: null argument");
     FD2_CHECK_CUDA(cudaStreamSynchronize(e->stream));
@@ -845,21 +924,21 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
     *out = nullptr;
     const std::string dir(folder);
     const bool half = value_type != FD2_VALUES_F32;
-    std::vector<char> b_nrows, b_off, b_col, b_val, b_nnz, b_scale;
+    const size_t vb = half ? 2 : 4;
+    // the per-matrix tables and the row offsets are small: read whole
+    std::vector<char> b_nrows, b_off, b_nnz, b_scale;
     FD2_TRY(read_file(dir + "/numRowsPerMat.bin", b_nrows));
     FD2_TRY(read_file(dir + "/NonZeroElements.bin", b_nnz));
     FD2_TRY(read_file(dir + "/offsetsBuffer.bin", b_off));
-    FD2_TRY(read_file(dir + "/columnsBuffer.bin", b_col));
+    std::string val_path = dir + "/valuesBuffer.bin";
     if (half) {
         // a 16-bit ensemble loads from the sidecars its tofile wrote; folders from
         // the reference (float32 only) load as F32 and are rounded by the VOI step
         FD2_REQUIRE(std::ifstream(dir + sidecar_values(value_type)).good(), FD2_ERR_NOT_SUPPORTED,
                     "fromfile: %s has no %s sidecar; load F32 and restrict with a 16-bit value type", folder,
                     sidecar_values(value_type).c_str() + 1);
-        FD2_TRY(read_file(dir + sidecar_values(value_type), b_val));
+        val_path = dir + sidecar_values(value_type);
         FD2_TRY(read_file(dir + sidecar_scales(value_type), b_scale));
-    } else {
-        FD2_TRY(read_file(dir + "/valuesBuffer.bin", b_val));
     }
     const size_t nm = b_nrows.size() / 8;
     FD2_REQUIRE(b_nnz.size() / 8 == nm, FD2_ERR_IO, "fromfile: NonZeroElements.bin has %zu entries, expected %zu",
@@ -867,11 +946,14 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
     const uint64_t* nrows = (const uint64_t*)b_nrows.data();
     const uint64_t* off = (const uint64_t*)b_off.data();
     const uint64_t* mnnz = (const uint64_t*)b_nnz.data();
-    const size_t nnz = b_col.size() / 8;
-    FD2_REQUIRE(b_val.size() / (half ? 2 : 4) == nnz, FD2_ERR_IO, "fromfile: values/columns size mismatch");
-    uint64_t total_rows = 0, check = 0;
-    for (size_t m = 0; m < nm; m++) { total_rows += nrows[m]; check += mnnz[m]; }
-    FD2_REQUIRE(check == nnz, FD2_ERR_IO, "fromfile: nnz mismatch");
+    uint64_t total_rows = 0, nnz = 0;
+    for (size_t m = 0; m < nm; m++) { total_rows += nrows[m]; nnz += mnnz[m]; }
+    struct stat sc{}, sv{};
+    const std::string col_path = dir + "/columnsBuffer.bin";
+    FD2_REQUIRE(stat(col_path.c_str(), &sc) == 0 && stat(val_path.c_str(), &sv) == 0, FD2_ERR_IO,
+                "fromfile: cannot stat the columns or values of %s", folder);
+    FD2_REQUIRE((uint64_t)sc.st_size == nnz * 8, FD2_ERR_IO, "fromfile: nnz mismatch");
+    FD2_REQUIRE((uint64_t)sv.st_size == nnz * vb, FD2_ERR_IO, "fromfile: values/columns size mismatch");
     FD2_REQUIRE(b_off.size() / 8 == total_rows + nm, FD2_ERR_IO, "fromfile: offsetsBuffer size mismatch");
     FD2_REQUIRE(!half || b_scale.size() / 4 == total_rows, FD2_ERR_IO, "fromfile: row scales size mismatch");
     std::vector<int64_t> ro(total_rows + 1, 0);
@@ -888,12 +970,6 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
         ob += nrows[m] + 1;
         mat_rows.push_back(r);
     }
-    const uint64_t* c64 = (const uint64_t*)b_col.data();
-    std::vector<int32_t> col(nnz);
-    for (size_t k = 0; k < nnz; k++) {
-        FD2_REQUIRE(c64[k] < n_cols, FD2_ERR_IO, "fromfile: column %llu out of range", (unsigned long long)c64[k]);
-        col[k] = (int32_t)c64[k];
-    }
     auto* e = new fd2_csr_ensemble();
     e->ctx = ctx;
     e->stream = ctx->stream;
@@ -901,17 +977,16 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
     e->value_type = value_type;
     e->mat_rows = mat_rows;
     int rc = ensemble_reserve(e, total_rows, nnz);
-    if (!rc && cudaStreamSynchronize(e->stream) != cudaSuccess) rc = FD2_ERR_CUDA;  // the arrays exist
+    if (!rc) rc = stream_columns(ctx, col_path, val_path, nnz, vb, n_cols, e->d_col, e->d_val, e->stream);
+    if (!rc && cudaMemcpyAsync(e->d_row_off, ro.data(), ro.size() * 8, cudaMemcpyHostToDevice, e->stream) != cudaSuccess)
+        rc = FD2_ERR_CUDA;
+    if (!rc && half && total_rows &&
+        cudaMemcpyAsync(e->d_scale, b_scale.data(), total_rows * 4, cudaMemcpyHostToDevice, e->stream) != cudaSuccess)
+        rc = FD2_ERR_CUDA;
+    if (!rc && cudaStreamSynchronize(e->stream) != cudaSuccess) rc = FD2_ERR_CUDA;
     if (!rc) {
-        cudaMemcpy(e->d_row_off, ro.data(), ro.size() * 8, cudaMemcpyHostToDevice);
-        if (nnz) {
-            cudaMemcpy(e->d_col, col.data(), nnz * 4, cudaMemcpyHostToDevice);
-            cudaMemcpy(e->d_val, b_val.data(), nnz * (half ? 2 : 4), cudaMemcpyHostToDevice);
-        }
-        if (half && total_rows) cudaMemcpy(e->d_scale, b_scale.data(), total_rows * 4, cudaMemcpyHostToDevice);
         e->n_rows = total_rows;
         e->nnz = e->nnz_bound = nnz;
-        if (cudaDeviceSynchronize() != cudaSuccess) rc = FD2_ERR_CUDA;
     }
     if (rc) {
         fd2_csr_ensemble_destroy(e);

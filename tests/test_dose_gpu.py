@@ -307,3 +307,51 @@ def test_host_copy_while_building(ctx, vt):
     np.testing.assert_array_equal(again.to_host()[0], ro_r)
     for mm in (ref, again):
         mm.close()
+
+
+def _write_folder(path, mats, vals_dtype=np.float32):
+    """A doseMatFolder (the reference's layout) from host CSR matrices."""
+    path.mkdir(parents=True, exist_ok=True)
+    nrows = np.array([len(ro) - 1 for ro, _, _ in mats], np.uint64)
+    nnz = np.array([ro[-1] for ro, _, _ in mats], np.uint64)
+    nrows.tofile(path / "numRowsPerMat.bin")
+    np.cumsum(nrows).astype(np.uint64).tofile(path / "CumuNumRowsPerMat.bin")
+    nnz.tofile(path / "NonZeroElements.bin")
+    np.cumsum(nnz).astype(np.uint64).tofile(path / "CumuNonZeroElements.bin")
+    np.concatenate([[0], np.cumsum(nrows + 1)[:-1]]).astype(np.uint64).tofile(path / "OffsetBufferIdx.bin")
+    np.concatenate([np.asarray(ro, np.uint64) for ro, _, _ in mats]).tofile(path / "offsetsBuffer.bin")
+    np.concatenate([np.asarray(c, np.uint64) for _, c, _ in mats]).tofile(path / "columnsBuffer.bin")
+    np.concatenate([np.asarray(v, vals_dtype) for _, _, v in mats]).tofile(path / "valuesBuffer.bin")
+
+
+def test_fromfile_streams_large_folders(ctx, tmp_path):
+    """A folder of 9.4M nonzeros in two matrices loads in several streamed
+    chunks: the same row offsets, columns and values as written.  A column
+    outside the volume is refused."""
+    rng = np.random.default_rng(21)
+    n_cols = 2_000_000
+    mats = []
+    for rows, per in ((300, 20_000), (170, 20_000)):
+        lens = rng.integers(per // 2, per * 3 // 2, rows)
+        ro = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        col = np.concatenate([np.sort(rng.integers(0, n_cols, l)) for l in lens]).astype(np.int64)
+        val = rng.random(ro[-1]).astype(np.float32)
+        mats.append((ro, col, val))
+    _write_folder(tmp_path / "big", mats)
+    m = api.MatCSREnsemble.fromfile(ctx, tmp_path / "big", n_cols)
+    ro, col, val = m.to_host()
+    assert m.info()["nnz"] == sum(int(x[0][-1]) for x in mats) > 8_400_000
+    ro_ref = np.concatenate([mats[0][0], mats[1][0][1:] + mats[0][0][-1]])
+    np.testing.assert_array_equal(ro, ro_ref)
+    np.testing.assert_array_equal(col, np.concatenate([mats[0][1], mats[1][1]]))
+    np.testing.assert_array_equal(val, np.concatenate([mats[0][2], mats[1][2]]))
+    np.testing.assert_array_equal(m.mat_rows(), [0, 300, 470])
+    m.close()
+    from fastdose_b200 import _lib
+
+    bad = [(mats[0][0], mats[0][1].copy(), mats[0][2])]
+    bad[0][1][-1] = n_cols  # one index past the volume, in the last chunk
+    _write_folder(tmp_path / "bad", bad)
+    with pytest.raises(_lib.FD2Error) as e:
+        api.MatCSREnsemble.fromfile(ctx, tmp_path / "bad", n_cols)
+    assert "outside" in str(e.value)
