@@ -141,6 +141,9 @@ int fd2_csr_ensemble_tofile(const fd2_csr_ensemble* e, const char* folder);
  * MatCSREnsemble::fromfile (IMRTSparseMatEns.cu:242-337) into a device ensemble.
  * value_type F32 reads valuesBuffer.bin; F16/BF16 read that type's sidecars
  * (the exact stored values and scales) and refuse a folder without them.
+ * Columns and values stream to the device in chunks of 4M nonzeros through
+ * two pinned host buffers (host memory stays at two chunks); a column index
+ * >= n_cols is refused with FD2_ERR_IO.
  */
 int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_cols,
                               int value_type, fd2_csr_ensemble** out);
