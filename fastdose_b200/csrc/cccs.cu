@@ -28,6 +28,8 @@
 // correctly rounded float operations in the order the reference writes them,
 // starting from cone directions computed on the host; the CPU oracle performs
 // the identical operations, so both march the same segments bit for bit.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -734,8 +736,10 @@ extern "C" int fd2_cccs_cone_directions(fd2_context* ctx, const fd2_cccs_kernel*
 // are set.  Those callers get this entry point: no context, no cudaMalloc, no
 // cudaFree, no allocating library.  What it needs beyond the caller's buffers
 // -- the status word and the direction table -- lives in one fixed array in
-// device global memory, defined below; its address is looked up once per
-// device with cudaGetSymbolAddress on the first call.
+// device global memory, defined below.  Its address belongs to the CUDA
+// context that loaded this library's device code, so it is looked up with
+// cudaGetSymbolAddress on the first call in each context (once per device
+// under the runtime's primary context) and kept under that context's id.
 //
 // Limits: n_beams * n_forward_theta * n_phi * 16 bytes of directions must fit
 // FD2_DOSE_STATIC_DIR_BYTES (256 KiB: 256 beams of an 8 x 8 cone kernel);
@@ -757,30 +761,71 @@ namespace {
 
 constexpr size_t kStaticStatusBytes = 256;  // fd2::DeviceStatus, padded to keep the table aligned
 constexpr size_t kStaticDirBytes = FD2_DOSE_STATIC_DIR_BYTES;
-constexpr int kStaticMaxDevices = 64;
 constexpr size_t kBeamChunk = 32;  // beam descriptors read back per copy, on the host stack
 static_assert(sizeof(fd2::DeviceStatus) <= kStaticStatusBytes, "status word outgrew its slot");
 
-void* g_static_addr[kStaticMaxDevices];
+// Looked-up addresses, one per CUDA context.  A context is named by its
+// driver-assigned id, which is never reused within a process: a second context
+// on the same device, or the primary context recreated after cudaDeviceReset,
+// gets a new id and so a fresh lookup (the module may load at another address).
+struct StaticAddr {
+    unsigned long long ctx_id;
+    void* addr;
+};
+std::vector<StaticAddr> g_static_addr;
 std::mutex g_static_mu;
 
-// The device address of fd2_static_scratch on the current device.  Host code
-// only sees a stand-in for the array's name, so the address is looked up with
-// cudaGetSymbolAddress, once per device, and cached.
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+CtxGetIdFn g_ctx_get_id = nullptr;
+std::once_flag g_ctx_fns_once;
+
+// The id of the context current on this thread; false when none is current
+// yet or the driver does not offer the query.  The driver functions come
+// through the runtime's entry-point table, so the library does not link the
+// driver library itself.
+bool current_context_id(unsigned long long* id) {
+    std::call_once(g_ctx_fns_once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_current = (CtxGetCurrentFn)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_ctx_get_id = (CtxGetIdFn)f;
+    });
+    if (!g_ctx_get_current || !g_ctx_get_id) return false;
+    CUcontext c = nullptr;
+    if (g_ctx_get_current(&c) != CUDA_SUCCESS || c == nullptr) return false;
+    return g_ctx_get_id(c, id) == CUDA_SUCCESS;
+}
+
+// The device address of fd2_static_scratch in the current context.  Host
+// code only sees a stand-in for the array's name, so the address is looked up
+// with cudaGetSymbolAddress (which also makes the device's primary context
+// current if none is) the first time a context calls, then reused.
 int static_scratch_address(unsigned char** out) {
-    int dev = 0;
-    FD2_CHECK_CUDA(cudaGetDevice(&dev));
-    FD2_REQUIRE(dev >= 0 && dev < kStaticMaxDevices, FD2_ERR_NOT_SUPPORTED,
-                "dose_compute_static: device ordinal %d beyond %d", dev, kStaticMaxDevices);
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    if (!g_static_addr[dev]) {
-        void* p = nullptr;
-        FD2_CHECK_CUDA(cudaGetSymbolAddress(&p, fd2_static_scratch));
-        FD2_REQUIRE(p != nullptr && ((uintptr_t)p & 255) == 0, FD2_ERR_CUDA,
-                    "dose_compute_static: scratch address %p not 256-byte aligned", p);
-        g_static_addr[dev] = p;
+    unsigned long long id = 0;
+    if (current_context_id(&id)) {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        for (const StaticAddr& s : g_static_addr)
+            if (s.ctx_id == id) {
+                *out = (unsigned char*)s.addr;
+                return FD2_OK;
+            }
     }
-    *out = (unsigned char*)g_static_addr[dev];
+    void* p = nullptr;
+    FD2_CHECK_CUDA(cudaGetSymbolAddress(&p, fd2_static_scratch));
+    FD2_REQUIRE(p != nullptr && ((uintptr_t)p & 255) == 0, FD2_ERR_CUDA,
+                "dose_compute_static: scratch address %p not 256-byte aligned", p);
+    if (current_context_id(&id)) {
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        g_static_addr.push_back({id, p});
+    }
+    *out = (unsigned char*)p;
     return FD2_OK;
 }
 

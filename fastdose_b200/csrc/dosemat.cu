@@ -921,6 +921,10 @@ int fd2_csr_ensemble_fromfile(fd2_context* ctx, const char* folder, uint64_t n_c
     FD2_REQUIRE(ctx && folder && out, FD2_ERR_INVALID_ARGUMENT, "fromfile: null argument");
     FD2_REQUIRE(value_type >= FD2_VALUES_F32 && value_type <= FD2_VALUES_BF16, FD2_ERR_INVALID_ARGUMENT,
                 "fromfile: value type %d", value_type);
+    // columns are held as int32 on the device: a volume of 2^31 voxels or more
+    // would let an index pass the range check and wrap negative
+    FD2_REQUIRE(n_cols <= (uint64_t)INT32_MAX, FD2_ERR_INVALID_ARGUMENT,
+                "fromfile: a %llu-voxel volume exceeds the int32 column range", (unsigned long long)n_cols);
     *out = nullptr;
     const std::string dir(folder);
     const bool half = value_type != FD2_VALUES_F32;

@@ -245,9 +245,12 @@ int fd2_dose_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_beams,
  * loads the library until exit), and nothing is allocated by cudaMalloc or
  * any library.
  *
- * - The first call on each device looks up that array's address (which may
- *   load the library's device code onto the device); make it during set-up,
- *   before any stream capture.
+ * - The array's address belongs to the CUDA context that loaded the
+ *   library's device code.  The first call in each context (once per device
+ *   under the runtime's primary context) looks it up, which may load that
+ *   device code; make that first call during set-up, before any stream
+ *   capture.  A second context on a device, or a context recreated after
+ *   cudaDeviceReset, gets its own lookup.
  * - Limit: n_beams * n_forward_theta * n_phi * 16 <= FD2_DOSE_STATIC_DIR_BYTES
  *   (256 beams of an 8 x 8 cone kernel); larger batches return
  *   FD2_ERR_CAPACITY before any device work.

@@ -355,3 +355,11 @@ def test_fromfile_streams_large_folders(ctx, tmp_path):
     with pytest.raises(_lib.FD2Error) as e:
         api.MatCSREnsemble.fromfile(ctx, tmp_path / "bad", n_cols)
     assert "outside" in str(e.value)
+    # an index of 2^31 would wrap negative as int32: a volume that large is
+    # refused before any column is read
+    huge = [(mats[1][0], mats[1][1].copy(), mats[1][2])]
+    huge[0][1][-1] = 2**31
+    _write_folder(tmp_path / "huge", huge)
+    with pytest.raises(_lib.FD2Error) as e:
+        api.MatCSREnsemble.fromfile(ctx, tmp_path / "huge", 2**31 + 1)
+    assert "int32" in str(e.value)
