@@ -8,9 +8,17 @@ oracle/build_ref.sh) on a GPU:
   dose_small_ref.npz  a small oblique case (all 16 beamlets)
   bev2pvcs_ref.npz    fastdose::BEV2PVCS of one beamlet's dose (texture path)
   flags_c2_ref.npz    beamletFlagInit of the 4pi torso bundles
+  dose_c2_ref.npz     the 4pi torso plan (config 2): two beamlets from each of
+                      six oblique beams -- Terma and dose BEV of the first,
+                      the interpolated dose column of both
+  bev2pvcs_ss_ref.npz fastdose::BEV2PVCS_SuperSampling of config-1 beamlet 44
+  reference_timings.json  kernel times, and IMRT::DoseMatConstruction's steps
+                      over the whole 4pi plan (part "c2full")
 
-Usage (on a GPU machine): python tests/golden/make_golden_dose.py OUTDIR
-The fixtures are then copied next to this script.
+Usage (on a GPU machine): python tests/golden/make_golden_dose.py OUTDIR [part ...]
+with parts from c1 small flags c2timing c2 ss c2full (default: all).  The
+fixtures are then copied next to this script; reference_timings.json is
+updated in place, keeping the keys of parts not rerun.
 """
 import json
 import os
@@ -142,19 +150,102 @@ def c2_timing(outdir, n_beams=8):
                 c2_ref_beamlets_per_s=tot_b / (tot_ms * 1e-3) if tot_ms else None)
 
 
+C2_PICK_BEAMS = (0, 67, 134, 201, 268, 335)
+
+
+def _c2_plan():
+    cfg = phantoms.config2()
+    bundles = np.array([make_bundle(cfg["isocenter"], a, sad=cfg["sad"], fluence_dim=cfg["fluence_dim"],
+                                    beamlet_size=cfg["beamlet_size"], sub_fluence_dim=cfg["sub_fluence_dim"],
+                                    sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+                        for a in cfg["angles"]])
+    fl = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "flags_c2_ref.npz"))["flags"]
+    return cfg, bundles, fl
+
+
+def c2(outdir):
+    """Sampled beamlets of the 4pi torso plan through the reference's Terma,
+    CCCS and batched interpolation (8x8 cone kernel)."""
+    from fastdose_b200 import api
+
+    cfg, bundles, fl = _c2_plan()
+    ph = cfg["phantom"]
+    kern = ref_kernel()
+    keep = {}
+    beams_all = []
+    for bi in C2_PICK_BEAMS:
+        beams = api.bundle_beamlets(bundles[bi], fl[bi], ph.volume)
+        assert len(beams) >= 2, (bi, len(beams))
+        sel = beams[[len(beams) // 2, 0]]
+        log("c2: beam", bi, "beamlets", len(beams), "picked long_dim", sel["long_dim"])
+        r = ref.dose_batch(sel, api.beamlet_fluence(bundles[bi]), ph.density, ph.volume, cfg["spectrum"], kern,
+                           extent=cfg["extent"], dense=True)
+        assert r["status"] == 0, r["status"]
+        j = len(beams_all)
+        L = int(sel[0]["long_dim"])
+        keep[f"terma_{j}"] = r["terma"][0, :L]
+        keep[f"dose_{j}"] = r["dose"][0, :L]
+        for k in range(2):
+            nz = np.nonzero(r["dense"][k])[0]
+            keep[f"col_{j + k}"] = nz.astype(np.int32)
+            keep[f"val_{j + k}"] = r["dense"][k, nz]
+        beams_all.extend(sel)
+    np.savez_compressed(os.path.join(outdir, "dose_c2_ref.npz"), beams=np.array(beams_all),
+                        beam_index=np.repeat(C2_PICK_BEAMS, 2), kernel_phi=kern.phi, **keep)
+
+
+def ss(outdir):
+    """BEV2PVCS_SuperSampling of config-1 beamlet 44's dose BEV."""
+    g = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "dose_c1_ref.npz"))
+    case = c1_case()
+    b = case["beams"][44]
+    bev = g["dose_44"]
+    out = {}
+    for ssf, ext in ((5, 2.0), (3, 0.6)):
+        st, vol = ref.bev2pvcs_ss(b, bev, case["phantom"].volume, ssfactor=ssf, extent=ext)
+        assert st == 0
+        out[f"out_{ssf}"] = vol
+    np.savez_compressed(os.path.join(outdir, "bev2pvcs_ss_ref.npz"), beam=b, **out)
+
+
+def c2full(outdir):
+    """IMRT::DoseMatConstruction's steps over the whole 4pi plan."""
+    cfg, bundles, fl = _c2_plan()
+    ph = cfg["phantom"]
+    t0 = time.time()
+    r = ref.dose_mat_steps(bundles, fl, ph.density, ph.volume, cfg["spectrum"], ref_kernel(), extent=cfg["extent"])
+    wall = time.time() - t0
+    assert r["status"] == 0, r["status"]
+    t = r["times_ms"]
+    log("c2full:", r["beamlets"], "beamlets", t, "ms, nnz", int(r["nnz"].sum()))
+    return dict(c2full_beamlets=int(r["beamlets"]), c2full_terma_ms=float(t[0]), c2full_cccs_ms=float(t[1]),
+                c2full_interp_ms=float(t[2]), c2full_dense_to_csr_ms=float(t[3]), c2full_total_ms=float(t[4]),
+                c2full_nnz=int(r["nnz"].sum()), c2full_wall_s=wall,
+                c2full_beamlets_per_s=r["beamlets"] / (float(t[4]) * 1e-3))
+
+
+PARTS = ("c1", "small", "flags", "c2timing", "c2", "ss", "c2full")
+
+
 def main():
     outdir = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.abspath(__file__))
+    parts = sys.argv[2:] or PARTS
     os.makedirs(outdir, exist_ok=True)
     if not ref.available():
         raise SystemExit("oracle/_ref/libfdref.so missing: run oracle/build_ref.sh")
     t0 = time.time()
+    path = os.path.join(outdir, "reference_timings.json")
     meta = {}
-    meta.update(c1(outdir))
-    small(outdir)
-    meta.update(flags(outdir))
-    meta.update(c2_timing(outdir))
+    if os.path.exists(path):
+        with open(path) as f:
+            meta = json.load(f)
+    fns = dict(c1=c1, small=small, flags=flags, c2timing=c2_timing, c2=c2, ss=ss, c2full=c2full)
+    for p in parts:
+        got = fns[p](outdir)
+        if got:
+            meta.update(got)
     meta["wall_s"] = time.time() - t0
-    with open(os.path.join(outdir, "reference_timings.json"), "w") as f:
+    with open(path, "w") as f:
         json.dump(meta, f, indent=1)
     print(json.dumps(meta))
 
