@@ -115,14 +115,40 @@ class ClockSampler:
         return out
 
 
-def cpu_baseline(cfg, beamlets, fluence, budget_s, threads):
-    """The CPU restatement (single-precision build) on host threads, over a
-    bounded sample of the plan's beamlets: beamlets/s."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
+def stratified_order(beamlets, every=10):
+    """Beamlet order for the CPU samples: beams 0, every, 2*every, ... taken
+    round-robin (one beamlet of each in turn), so consecutive samples spread
+    over the sphere of beams; the plan's other beams follow."""
+    groups = [list(range(sum(len(b) for b in beamlets[:i]), sum(len(b) for b in beamlets[:i + 1])))
+              for i in range(len(beamlets))]
+    picked = [g for i, g in enumerate(groups) if i % every == 0 and g]
+    order = []
+    depth = 0
+    while any(depth < len(g) for g in picked):
+        order += [g[depth] for g in picked if depth < len(g)]
+        depth += 1
+    rest = [k for i, g in enumerate(groups) if i % every != 0 for k in g]
+    return np.array(order + rest, np.int64)
+
+
+def cpu_baseline(cfg, beamlets, fluence, budget_s, threads, start=0, order=None):
+    """The CPU restatement (single-precision build) on host threads over a
+    bounded sample of the plan's beamlets, taken in `order` from position
+    `start`: beamlets/s, and where the next sample should start."""
     import oracle
 
     flat = np.concatenate(beamlets)
-    rng = np.random.default_rng(0)
-    order = rng.permutation(len(flat))
+    order = stratified_order(beamlets) if order is None else order
     ph = cfg["phantom"]
     done = 0
     t0 = time.perf_counter()
@@ -130,13 +156,14 @@ def cpu_baseline(cfg, beamlets, fluence, budget_s, threads):
 
     with ThreadPoolExecutor(threads) as ex:
         while time.perf_counter() - t0 < budget_s and done < len(flat):
-            chunk = flat[order[done:done + threads]]
+            idx = order[(start + done + np.arange(threads)) % len(flat)]
             list(ex.map(lambda b: oracle.beamlet_pipeline(b, fluence, ph.density, ph.volume, cfg["spectrum"],
-                                                          cfg["kernel"], precision="float"), chunk))
-            done += len(chunk)
+                                                          cfg["kernel"], precision="float"), flat[idx]))
+            done += len(idx)
     dt = time.perf_counter() - t0
-    return {"value": done / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{done} of {len(flat)} beamlets of the same plan (Terma, CCCS, column), {dt:.1f} s"}
+    return {"value": done / dt, "unit": UNIT, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
+            "sample": f"{done} of {len(flat)} beamlets of the same plan (Terma, CCCS, column), {dt:.1f} s, "
+                      f"taken round-robin from every 10th beam"}, start + done
 
 
 def workload_name(n_beams, n_beamlets):
@@ -145,43 +172,60 @@ def workload_name(n_beams, n_beamlets):
             f"8x6 cones, 12-bin spectrum")
 
 
+def oracle_plan_beamlets(bundles, ptv_mask, volume):
+    """The plan's beamlets from the oracle alone (no CUDA library): the host
+    restatement of the PTV flag test (texture weights emulated) and of
+    beamletInit, in the reference's order (pixels row by row, beams in turn)."""
+    import oracle
+
+    beams0 = np.array([oracle.calc_range(_bundle_beam(b), volume)[1] for b in bundles])
+    flags = oracle.beamlet_flags(beams0, ptv_mask, volume, tex_mode=1, precision="float")
+    out = []
+    for bb, fl in zip(bundles, flags):
+        fx, fy = (int(v) for v in bb["fluence_dim"])
+        got = []
+        for j in range(fy):
+            for i in range(fx):
+                if fl[i + j * fx]:
+                    st, b = oracle.beamlet_init(bb, i, j, volume)
+                    got.append(b)
+        out.append(np.array(got) if got else np.zeros(0, beams0.dtype))
+    return out
+
+
 def run_reference(args, rank):
     """--impl reference: the reference has no CPU implementation of this path;
-    its algorithm is timed through the CPU restatement on all host cores."""
+    its algorithm is timed through the CPU restatement on all host cores.
+    Only oracle/ code runs here: the plan's geometry and flags come from the
+    oracle's host restatements, not from this library."""
     if rank != 0:
         return
-    from fastdose_b200 import api
+    import oracle
 
     cfg, bundles = plan_inputs(args.beams * max(1, args.gpus))
     ph = cfg["phantom"]
-    # beam selection as in the fd2 arm: PTV-flagged beamlets (host restatement of the flag test)
-    import oracle
-
-    flags = None
-    try:
-        ctx = api.Context(0)
-        flags = api.beamletFlagInit(ctx, bundles, ph.masks["PTV"], ph.volume)
-    except Exception:
-        flags = None
-    if flags is None:
-        beams0 = np.array([api.calc_range(_bundle_beam(b), ph.volume) for b in bundles])
-        flags = oracle.beamlet_flags(beams0, ph.masks["PTV"], ph.volume, tex_mode=1)
-    beamlets = api.bundles_beamlets(bundles, flags, ph.volume)
+    beamlets = oracle_plan_beamlets(bundles, ph.masks["PTV"], ph.volume)
     n_bl = int(sum(len(b) for b in beamlets))
-    fluence = api.beamlet_fluence(bundles[0])
+    fluence = oracle.beamlet_fluence(bundles[0])
     threads = os.cpu_count() or 1
+    order = stratified_order(beamlets)
     steps = []
+    pos = 0
+    # each step a bounded sample; the whole run stays near 2.5 minutes
+    per_step = min(args.cpu_seconds, max(2.0, 150.0 / (args.warmup + args.steps)))
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, threads)
+        r, pos = cpu_baseline(cfg, beamlets, fluence, per_step, threads, start=pos, order=order)
         if i >= args.warmup:
             steps.append(r["value"])
     v = statistics.median(steps)
+    r["sample"] += f"; {pos} beamlets over {args.warmup + args.steps} steps, median of the timed steps"
     line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": workload_name(len(bundles), n_bl), "beams": len(bundles), "beamlets": n_bl,
                        "parallelism": f"CPU restatement on {threads} host threads"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": r["sample"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "cpu_model": r["cpu_model"], "kind": "port",
+                             "sample": r["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -265,7 +309,8 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
     x0 = torch.full((cols,), 0.01, dtype=torch.float32, device="cuda")
     # the FP32 matrix and plan are kept to dose every format's plan exactly:
     # DVHs of the PTV and OAR rows against the FP32-optimized plan's
-    A32 = x32 = dvh32 = None
+    A32 = x32 = dvh32 = P32 = None
+    finals = {}
     structures = [np.arange(n_ptv), np.arange(n_ptv, rows)]
     n_bins = 200
     for vt, fmt in (("f32", "i32"), ("f32", "packed16"), ("f16", "packed16"), ("bf16", "packed16")):
@@ -298,8 +343,9 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
                    "spmv": spmv_a, "spmv_transpose": spmv_at}
         if key == "f16_packed16":
             out[key]["it_per_s_without_graph"] = graph_off_it_s
+        finals[key] = r["x"].clone()
         if A32 is None:
-            A32, x32 = A, r["x"].clone()
+            A32, x32, P32 = A, r["x"].clone(), P
             dose32 = A32.spmv(x32)
             width = float(dose32.max().item()) / (n_bins - 1)
             _, dvh32 = optimize.dvh(ctx, dose32, structures, n_bins, width)
@@ -307,18 +353,115 @@ def optimizer_leg(ctx, iters, rows=2_500_000, n_beams=400, seed=3):
         else:
             _, dvh_k = optimize.dvh(ctx, A32.spmv(r["x"]), structures, n_bins, width)
             out[key]["dvh_max_abs_diff_vs_f32"] = float(np.abs(dvh_k - dvh32).max())
-        del P, AT
+        if P is not P32:
+            del P, AT
         if A is not A32:
             del A
         torch.cuda.empty_cache()
-    del A32, x32
+    # every format's plan scored on the FP32 matrix (FP32 products, FP64 sums)
+    for key, xk in finals.items():
+        out[key]["objective_on_f32_matrix"] = P32.eval_g(xk)
+    base_obj = out["f32_i32"]["objective_on_f32_matrix"]
+    for key in finals:
+        out[key]["objective_on_f32_matrix_rel_diff"] = abs(out[key]["objective_on_f32_matrix"] - base_obj) / abs(base_obj)
+    del A32, x32, P32, finals
+    torch.cuda.empty_cache()
     out["reference_form"] = reference_form_spmv(ctx, rows // 10, cols, seed, peak)
+    out["reference_cuda"] = reference_optimizer_leg(ctx, rows // 10, n_beams, fd, seed)
     base = out["f32_i32"]
     for key in ("f32_packed16", "f16_packed16", "bf16_packed16"):
         out[key]["speedup_vs_f32_i32"] = out[key]["it_per_s"] / base["it_per_s"]
         out[key]["objective_rel_diff_vs_f32"] = abs(out[key]["loss"] - base["loss"]) / abs(base["loss"])
     for key in ("f16_packed16", "bf16_packed16"):
         out[key]["speedup_vs_f32_packed16"] = out[key]["it_per_s"] / out["f32_packed16"]["it_per_s"]
+    return out
+
+
+def reference_optimizer_leg(ctx, rows, n_beams, fd, seed, iters=40, cpu_seconds=10.0):
+    """The reference's own GPU optimizer (BOO_IMRT_L2OneHalf_gpu_QL with its
+    eval_g / eval_grad / proxL2Onehalf_QL_gpu over cuSPARSE and cuBLAS,
+    IMRTOptimize.cu:16-194, compiled for sm_100a in oracle/_ref/libfdref.so)
+    on a tenth of the optimization matrix's rows, beside this library's BOO
+    in FP32 and FP16 on the same matrix and weights; and the CPU restatement
+    of the same loop (the oracle's single-precision build, one host thread,
+    a bounded number of iterations) as the CPU baseline.  A baseline leg:
+    nothing here is this library's product path."""
+    import torch
+
+    import oracle
+    from fastdose_b200 import optimize
+    from oracle import ref
+
+    cols = n_beams * fd * fd
+    window, density = rows // 25, 0.5
+    n_ptv = rows // 10
+    n_oar = rows - n_ptv
+    rng = np.random.default_rng(seed)
+    w = dict(max_dose=np.concatenate([np.ones(n_ptv), rng.uniform(0.3, 0.7, n_oar)]).astype(np.float32),
+             max_weights=np.concatenate([np.ones(n_ptv), rng.uniform(0.1, 1.0, n_oar)]).astype(np.float32),
+             min_dose=np.ones(n_ptv, np.float32), min_weights=np.ones(n_ptv, np.float32),
+             oar_weights=rng.uniform(0.0, 0.1, n_oar).astype(np.float32))
+    D = optimize.block_diag([optimize.fluence_grad(fd, np.ones(fd * fd, np.uint8))] * n_beams)
+    Dm = optimize.Matrix.from_csr(ctx, *D[:3], cols)
+    DTm = Dm.transpose()
+    groups = np.arange(0, cols + 1, fd * fd, dtype=np.int64)
+    out = {"workload": f"synthetic VOI matrix {rows}x{cols} (PTV {n_ptv}), window {window}, density {density}; "
+                       f"{iters} BOO iterations from x = 0.01, beam weight 0.1, gamma 1, eta 0.1"}
+    res = {}
+    for vt, fmt in (("f32", "i32"), ("f16", "packed16")):
+        A, AT = optimize.Matrix.synthetic(ctx, rows, cols, window, density, seed=seed, value_type=vt, index_format=fmt)
+        P = optimize.Problem(ctx, A, AT, Dm, DTm, n_ptv, n_oar, w["max_dose"], w["max_weights"], w["min_dose"],
+                             w["min_weights"], w["oar_weights"], 1.0, 0.1)
+        bw = 0.1 * P.beam_weights_init(groups)
+        x0 = np.full(cols, 0.01, np.float32)
+        P.boo(groups, bw, x0, step_size=1e-3, iters=3, want=0, change_trigger=10 ** 9)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        r = P.boo(groups, bw, x0, step_size=1e-3, iters=iters, want=0, change_trigger=10 ** 9)
+        dt = time.perf_counter() - t0
+        res[f"fd2_{vt}_{fmt}"] = {"it_per_s": r["k"] / dt, "loss": float(r["loss"][r["k"] - 1])}
+        if vt == "f32":
+            host = [A.to_host(), AT.to_host()]
+            bw32 = bw
+        del P, A, AT
+        torch.cuda.empty_cache()
+    (a_off, a_col, a_val), (t_off, t_col, t_val) = host
+    Ah = (a_off, a_col.astype(np.int64), a_val, cols)
+    ATh = (t_off, t_col.astype(np.int64), t_val, rows)
+    Dt = optimize.block_diag([optimize.fluence_grad(fd, np.ones(fd * fd, np.uint8))] * n_beams)
+    masks = np.ones((n_beams, fd * fd), np.uint8)
+    x0 = np.full(cols, 0.01, np.float32)
+    if ref.available():
+        R = ref.OptProblem(Ah, Dt, n_ptv, n_oar, w["max_dose"], w["max_weights"], w["min_dose"], w["min_weights"],
+                           w["oar_weights"], 1.0, 0.1, AT=ATh)
+        R.boo(masks, bw32, x0, x0, 1e-3, 3, want=0, change_trigger=10 ** 9)
+        t0 = time.perf_counter()
+        rr = R.boo(masks, bw32, x0, x0, 1e-3, iters, want=0, change_trigger=10 ** 9)
+        dt = time.perf_counter() - t0
+        R.close()
+        res["reference_f32_i64"] = {"it_per_s": rr["k"] / dt, "loss": float(rr["loss"][rr["k"] - 1]),
+                                    "note": "cuSPARSE SpMV on FP32 values with int64 indices, cuBLAS reductions "
+                                            "with host scalars (about 15 host synchronisations per trial)"}
+        for key in ("fd2_f32_i32", "fd2_f16_packed16"):
+            res[key]["speedup_vs_reference"] = res[key]["it_per_s"] / res["reference_f32_i64"]["it_per_s"]
+    else:
+        res["reference_f32_i64"] = {"unavailable": "oracle/_ref/libfdref.so is not built"}
+    # CPU baseline: the oracle's single-precision BOO, one host thread, bounded
+    O = oracle.Problem(Ah, Dt, n_ptv, n_oar, w["max_dose"], w["max_weights"], w["min_dose"], w["min_weights"],
+                       w["oar_weights"], 1.0, 0.1, precision="float", AT=ATh)
+    n_cpu, t0 = 0, time.perf_counter()
+    state = None
+    while n_cpu < iters and time.perf_counter() - t0 < cpu_seconds:
+        rc = O.boo(groups, bw32, x0 if state is None else rc["x"], 1e-3, n_cpu + 1, want=0, change_trigger=10 ** 9,
+                   state=state)
+        state = (rc["k"], rc["theta"], rc["t"], rc["v"])
+        n_cpu = rc["k"]
+    dt = time.perf_counter() - t0
+    out["cpu_baseline"] = {"value": n_cpu / dt, "unit": "BOO iterations/s", "cores": 1, "cpu_model": cpu_model(),
+                           "kind": "port", "sample": f"{n_cpu} iterations of the same problem, {dt:.1f} s"}
+    out.update(res)
+    del Dm, DTm
+    torch.cuda.empty_cache()
     return out
 
 
@@ -472,20 +615,25 @@ def c4_leg(ctx, n_per_iso=300, opt_iters=20):
     return out
 
 
-def served_requests(ctx, n_requests, seed=11):
+def served_requests(ctx, n_requests, seed=11, n_phantoms=24):
     """Seeded plan requests of the served benchmark: a torso phantom whose
     sides are drawn from 96..256 voxels (2.5 mm), 1..50 beams from the 4pi
-    sphere, 16x16 beamlet maps masked to the PTV."""
+    sphere, 16x16 beamlet maps masked to the PTV.  The phantoms come from a
+    pool of n_phantoms (each request draws its own beams), which keeps the
+    request set cheap to build on the host."""
     from fastdose_b200 import api, phantoms
     from fastdose_b200.types import make_bundle
 
     rng = np.random.default_rng(seed)
     angles = phantoms.sphere_beam_angles(400)
-    reqs = []
-    for i in range(n_requests):
+    pool = []
+    for i in range(min(n_phantoms, n_requests)):
         dim = tuple(int(v) for v in rng.integers(96, 257, size=3))
         ph = phantoms.torso_phantom(seed=100 + i, dim=dim, ptv_radius=2.5, ptv_offset=(1.5, 1.0, 0.0))
-        iso = phantoms.mask_centroid(ph.masks["PTV"], ph.voxel)
+        pool.append((ph, phantoms.mask_centroid(ph.masks["PTV"], ph.voxel)))
+    reqs = []
+    for i in range(n_requests):
+        ph, iso = pool[int(rng.integers(0, len(pool)))]
         sel = rng.choice(len(angles), size=int(rng.integers(1, 51)), replace=False)
         bundles = np.array([make_bundle(iso, angles[j], sad=100.0, fluence_dim=16, beamlet_size=0.5,
                                         sub_fluence_dim=16, sub_fluence_on=4, long_spacing=0.25) for j in sel])
@@ -496,12 +644,22 @@ def served_requests(ctx, n_requests, seed=11):
     return reqs
 
 
-def served_leg(ctx, rates=(2.0, 10.0), n_requests=16, seed=11, workers=2):
+def _lat_stats(lat_s):
+    lat = 1e3 * np.asarray(lat_s, np.float64)
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "max_ms": float(lat.max()), "requests": int(lat.size)}
+
+
+def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_per_rate=20.0, seed=11, workers=2,
+               plain_requests=30):
     """p50/p99 plan latency (arrival -> dose-loading matrix on the device) and
-    beamlets/s of the service under Poisson arrivals, and of the plain form --
-    the same requests one beam per construction call, one request at a time --
-    replayed through the same arrivals as a FIFO single server with its
-    measured service times."""
+    beamlets/s of the service under Poisson arrivals at each rate, over
+    min(n_requests, max(30, rate * seconds_per_rate)) requests (seconds_per_rate
+    0: n_requests at every rate); and of the plain form -- one request at a
+    time, one beam per construction call -- run live at 1 request/s over the
+    first plain_requests requests.  At higher rates the plain single server is
+    overloaded (its utilisation, rate x mean service time, is reported); its
+    latencies there are a FIFO replay of the service times measured live."""
     import threading
 
     import torch
@@ -511,50 +669,62 @@ def served_leg(ctx, rates=(2.0, 10.0), n_requests=16, seed=11, workers=2):
     spec, kern = phantoms.synthetic_spectrum(), phantoms.synthetic_kernel()
     reqs = served_requests(ctx, n_requests, seed)
     n_bl = [sum(len(b) for b in r["beams"]) for r in reqs]
-    out = {"workload": f"{len(reqs)} requests: torso sides U[96,256] at 2.5 mm, 1-50 beams, 16x16 PTV-masked "
-                       f"beamlets ({sum(n_bl)} beamlets), 8x6 cones; Poisson arrivals",
+    out = {"workload": f"{len(reqs)} requests: torso sides U[96,256] at 2.5 mm (a pool of 24 phantoms), 1-50 beams, "
+                       f"16x16 PTV-masked beamlets ({sum(n_bl)} beamlets), 8x6 cones; Poisson arrivals",
            "beamlets": int(sum(n_bl))}
-    # plain form: measured service time of each request, one beam per call
+    rng = np.random.default_rng(seed + 1)
+
+    # ---- the plain form, live: a single server, one beam per call, 1 request/s
     kk, ss = api.Kernel(ctx, kern), api.Spectrum(ctx, spec)
     st = torch.cuda.current_stream()
-    service_s = []
-    for r in reqs:
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
+    n_plain = min(plain_requests, len(reqs))
+
+    def plain_run(r):
         d = api.Density(ctx, r["phantom"].density, r["phantom"].volume)
         for b in r["beams"]:
             api.DoseMatConstruction(ctx, [b], r["fluence"], d, ss, kk, stream=st).close()
+        d.close()
         torch.cuda.synchronize()
-        service_s.append(time.perf_counter() - t0)
-    rng = np.random.default_rng(seed + 1)
+
+    plain_run(reqs[0])  # warm
+    arrivals = np.cumsum(rng.exponential(1.0, size=n_plain))
+    t0 = time.perf_counter()
+    lat, service_s = [], []
+    for a, r in zip(arrivals, reqs[:n_plain]):
+        now = time.perf_counter() - t0
+        if now < a:
+            time.sleep(a - now)
+        s0 = time.perf_counter()
+        plain_run(r)
+        end = time.perf_counter()
+        service_s.append(end - s0)
+        lat.append(end - t0 - a)
+    mean_s = float(np.mean(service_s))
+    plain_live = dict(_lat_stats(lat), rate_per_s=1.0, beamlets_per_s=sum(n_bl[:n_plain]) / (time.perf_counter() - t0),
+                      mean_service_ms=1e3 * mean_s)
+    out["plain_live_1_per_s"] = plain_live
+
+    svc = service.Service(device=torch.cuda.current_device(), workers=workers)
+    big = int(np.argmax(n_bl))
+    warmed = set()
+    for _ in range(4 * workers):  # until every worker has run the largest request once
+        tickets = [svc.submit(reqs[big]["phantom"], reqs[big]["beams"], reqs[big]["fluence"], spec, kern)
+                   for _ in range(workers)]
+        for t in tickets:
+            m, s = svc.wait(t)
+            m.close()
+            warmed.add(int(s["worker"]))
+        if len(warmed) == workers:
+            break
     for lam in rates:
-        arrivals = np.cumsum(rng.exponential(1.0 / lam, size=len(reqs)))
-        # the plain form as a FIFO single server
-        end, lat = 0.0, []
-        for a, s in zip(arrivals, service_s):
-            end = max(end, a) + s
-            lat.append(end - a)
-        plain = {"p50_ms": 1e3 * float(np.percentile(lat, 50)), "p99_ms": 1e3 * float(np.percentile(lat, 99)),
-                 "beamlets_per_s": sum(n_bl) / (end - arrivals[0])}
-        # the service, warmed by one untimed request per worker (a long-running
-        # service has its contexts and resident buffers in place)
-        svc = service.Service(device=torch.cuda.current_device(), workers=workers)
-        big = int(np.argmax(n_bl))
-        warmed = set()
-        for _ in range(4 * workers):  # until every worker has run the largest request once
-            tickets = [svc.submit(reqs[big]["phantom"], reqs[big]["beams"], reqs[big]["fluence"], spec, kern)
-                       for _ in range(workers)]
-            for t in tickets:
-                m, s = svc.wait(t)
-                m.close()
-                warmed.add(int(s["worker"]))
-            if len(warmed) == workers:
-                break
-        tickets = [None] * len(reqs)
+        n = len(reqs) if seconds_per_rate <= 0 else min(len(reqs), max(30, int(lam * seconds_per_rate)))
+        sub = reqs[:n]
+        arr = np.cumsum(rng.exponential(1.0 / lam, size=n))
+        tickets = [None] * n
         t_base = svc.clock_ms()
 
         def submitter():
-            for i, (a, r) in enumerate(zip(arrivals, reqs)):
+            for i, (a, r) in enumerate(zip(arr, sub)):
                 delay = t_base + 1e3 * a - svc.clock_ms()
                 if delay > 0:
                     time.sleep(delay * 1e-3)
@@ -569,20 +739,33 @@ def served_leg(ctx, rates=(2.0, 10.0), n_requests=16, seed=11, workers=2):
                 m, s = svc.wait(t)
                 m.close()
                 stats.append(s)
-        svc.close()
-        lat = np.array([s["end_ms"] - s["submit_ms"] for s in stats])
+        lat = np.array([s["end_ms"] - s["submit_ms"] for s in stats]) * 1e-3
         span_s = (max(s["end_ms"] for s in stats) - min(s["submit_ms"] for s in stats)) * 1e-3
-        out[f"rate_{lam:g}_per_s"] = {
-            "service": {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
-                        "queue_p50_ms": float(np.percentile([s["start_ms"] - s["submit_ms"] for s in stats], 50)),
-                        "beamlets_per_s": sum(n_bl) / span_s, "workers": workers,
-                        # per request (arrival order): beamlets, worker, submit ms (from the first
-                        # submit), queue ms, run ms
-                        "requests": [[int(s["beamlets"]), int(s["worker"]), round(s["submit_ms"] - stats[0]["submit_ms"], 1),
-                                      round(s["start_ms"] - s["submit_ms"], 1), round(s["end_ms"] - s["start_ms"], 1)]
-                                     for s in stats],
-                        "clocks": clk.summary()},
-            "plain_single_beam": plain}
+        # the plain single server at this rate: FIFO replay of the live service times
+        end, rl = 0.0, []
+        arr_p = arr[:n_plain]
+        for a, sv in zip(arr_p, service_s):
+            end = max(end, a) + sv
+            rl.append(end - a)
+        key = f"rate_{lam:g}_per_s"
+        out[key] = {
+            "service": dict(_lat_stats(lat), beamlets_per_s=sum(n_bl[:n]) / span_s, workers=workers,
+                            queue_p50_ms=float(np.percentile([s["start_ms"] - s["submit_ms"] for s in stats], 50)),
+                            # per request (arrival order): beamlets, worker, submit ms (from the first
+                            # submit), queue ms, run ms
+                            timeline=[[int(s["beamlets"]), int(s["worker"]),
+                                       round(s["submit_ms"] - stats[0]["submit_ms"], 1),
+                                       round(s["start_ms"] - s["submit_ms"], 1), round(s["end_ms"] - s["start_ms"], 1)]
+                                      for s in stats],
+                            clocks=clk.summary()),
+            "plain_single_beam": dict(_lat_stats(rl), utilisation=lam * mean_s,
+                                      basis="live" if lam == 1.0 else
+                                      f"FIFO replay of the {n_plain} live service times at this rate"),
+        }
+        if lam == 1.0:
+            out[key]["plain_single_beam"].update({k: plain_live[k] for k in ("p50_ms", "p99_ms", "max_ms")},
+                                                 basis="live")
+    svc.close()
     return out
 
 
@@ -605,6 +788,71 @@ def single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream, n_beams=20
     torch.cuda.synchronize()
     n = int(sum(len(b) for b in sel))
     return {"beams": len(sel), "beamlets": n, "value": n / (e0.elapsed_time(e1) * 1e-3), "unit": UNIT}
+
+
+def reference_cuda_leg(ctx, cfg, bundles, flags, all_beamlets, fluence, dens, spec, stream, value_8x6, every=8):
+    """The reference's own CUDA build on this B200 (oracle/_ref/libfdref.so:
+    its sources compiled unmodified for sm_100a) beside this library, both on
+    the 8x8 cone kernel of the same seed: IMRT::DoseMatConstruction's per-beam
+    steps (Terma, CCCS, BEV2PVCSInterp into the dense matrix, cuSPARSE
+    dense-to-CSR; one beam at a time, as its loop runs) over every
+    `every`-th beam of the plan, and this library on the same beams -- batched
+    in one call, and one beam per call -- and batched on the whole plan.
+    The reference's march with the plan's 8x6 kernel never ends (a cone at
+    phi = 90 degrees has a zero direction component in its fast-math build),
+    so the comparison uses 8 azimuths.  A baseline leg: nothing here is this
+    library's product path."""
+    import torch
+
+    from fastdose_b200 import api, phantoms
+    from oracle import ref
+
+    if not ref.available():
+        return {"unavailable": "oracle/_ref/libfdref.so is not built (oracle/build_ref.sh needs the reference sources)"}
+    ph = cfg["phantom"]
+    k88 = phantoms.synthetic_kernel(n_theta=8, n_phi=8)
+    sel = [i for i in range(0, len(bundles), every) if len(all_beamlets[i])]
+    r = ref.dose_mat_steps(bundles[sel], flags[sel], ph.density, ph.volume, cfg["spectrum"], k88, extent=cfg["extent"])
+    if r["status"] != 0:
+        return {"unavailable": f"reference DoseMatConstruction steps returned {r['status']}"}
+    t = r["times_ms"]
+    out = {"sample": f"every {every}th beam of the plan: {len(sel)} beams, {int(r['beamlets'])} beamlets, 8x8 cones",
+           "reference": {"beamlets_per_s": r["beamlets"] / (float(t[4]) * 1e-3), "ms": float(t[4]),
+                         "stage_ms": {"terma": float(t[0]), "cccs": float(t[1]), "interp": float(t[2]),
+                                      "dense_to_csr": float(t[3])},
+                         "nnz": int(r["nnz"].sum()),
+                         "note": "IMRTDoseMat.cu:183-259 run step by step by oracle/ref/ref_harness.cu; the "
+                                 "supervoxel flag array gets slack (its kernel writes past it on volumes that are "
+                                 "not a multiple of 32 voxels) and the BEV dose is cleared between beams"}}
+    kern88 = api.Kernel(ctx, k88)
+    beams_sel = [all_beamlets[i] for i in sel]
+
+    def timed(fn, reps=1):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    n_sel = int(sum(len(b) for b in beams_sel))
+    ms_b = timed(lambda: api.DoseMatConstruction(ctx, beams_sel, fluence, dens, spec, kern88, stream=stream).close(), 2)
+    ms_1 = timed(lambda: [api.DoseMatConstruction(ctx, [b], fluence, dens, spec, kern88, stream=stream).close()
+                          for b in beams_sel])
+    n_all = int(sum(len(b) for b in all_beamlets))
+    ms_all = timed(lambda: api.DoseMatConstruction(ctx, all_beamlets, fluence, dens, spec, kern88,
+                                                   stream=stream).close(), 2)
+    out["fd2"] = {"batched_beamlets_per_s": n_sel / (ms_b * 1e-3), "per_beam_beamlets_per_s": n_sel / (ms_1 * 1e-3),
+                  "whole_plan_batched_beamlets_per_s": n_all / (ms_all * 1e-3),
+                  "whole_plan_8x6_beamlets_per_s": value_8x6}
+    refv = out["reference"]["beamlets_per_s"]
+    out["speedup_vs_reference"] = {"batched_same_beams": out["fd2"]["batched_beamlets_per_s"] / refv,
+                                   "per_beam_same_beams": out["fd2"]["per_beam_beamlets_per_s"] / refv,
+                                   "whole_plan_batched": out["fd2"]["whole_plan_batched_beamlets_per_s"] / refv}
+    return out
 
 
 def run_fd2(args, rank, world):
@@ -780,7 +1028,12 @@ def run_fd2(args, rank, world):
         sb = single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream)
         sb["batched_speedup"] = value / world / sb["value"]
         line["single_beam"] = sb
+        if world == 1:
+            line["reference_cuda"] = reference_cuda_leg(ctx, cfg, bundles, flags, all_beamlets, fluence, dens, spec,
+                                                        stream, value)
         line["optimizer"] = optimizer_leg(ctx, args.opt_iters, args.opt_rows)
+        if world == 1:
+            line["c4"] = c4_leg(ctx)
         # the service's worker contexts start from a device the earlier legs
         # have handed back, as a service process would find it
         import gc
@@ -788,9 +1041,10 @@ def run_fd2(args, rank, world):
         gc.collect()
         torch.cuda.empty_cache()
         ctx.release()
-        line["served"] = served_leg(ctx)
+        line["served"] = served_leg(ctx, n_requests=args.served_requests, seconds_per_rate=args.served_seconds,
+                                    workers=args.served_workers)
     if rank == 0 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, os.cpu_count() or 1)
+        line["cpu_baseline"] = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, os.cpu_count() or 1)[0]
     if rank == 0:
         print(json.dumps(line), flush=True)
 
@@ -805,13 +1059,17 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the single-beam and optimizer legs")
-    ap.add_argument("--opt-iters", type=int, default=40)
+    ap.add_argument("--opt-iters", type=int, default=500)
     ap.add_argument("--opt-rows", type=int, default=2_500_000)
     ap.add_argument("--only-optimizer", action="store_true", help="run the optimizer leg alone (profiling)")
     ap.add_argument("--only-spmv", default=None, choices=["f32_i32", "f32_packed16", "f16_packed16", "bf16_packed16"],
                     help="time A x and A^T y of the optimization matrix in one format (profiling)")
     ap.add_argument("--spmv-reps", type=int, default=10)
     ap.add_argument("--served-workers", type=int, default=2)
+    ap.add_argument("--served-requests", type=int, default=200)
+    ap.add_argument("--served-seconds", type=float, default=20.0,
+                    help="arrival seconds per rate (caps the requests at low rates); 0: all requests at every rate")
+    ap.add_argument("--plain-requests", type=int, default=30, help="requests of the live plain-form run")
     ap.add_argument("--e2e-batch", type=int, default=-1,
                     help="beamlets per construction batch of the end-to-end leg (-1: a sixth of the plan, >= 4096)")
     ap.add_argument("--c4", action="store_true", help="run the multi-isocentre configuration alone")
@@ -844,7 +1102,10 @@ def main():
         if args.only_optimizer:
             print(json.dumps({"optimizer": optimizer_leg(ctx, args.opt_iters, args.opt_rows)}), flush=True)
         else:
-            print(json.dumps({"served": served_leg(ctx, workers=args.served_workers)}), flush=True)
+            print(json.dumps({"served": served_leg(ctx, n_requests=args.served_requests,
+                                                   seconds_per_rate=args.served_seconds,
+                                                   workers=args.served_workers, plain_requests=args.plain_requests)}),
+                  flush=True)
         return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -275,10 +275,11 @@ class Problem:
     """Optimizer inputs: A (VOI x beamlets), D (fluence-gradient rows), weights."""
 
     def __init__(self, A, D, n_ptv, n_oar, max_dose, max_weights, min_dose, min_weights, oar_weights,
-                 gamma, eta, precision="double"):
+                 gamma, eta, precision="double", AT=None):
         self.keep = []
         self.A, self.D = A, D
-        AT, DT = csr_transpose(A), csr_transpose(D)
+        AT = csr_transpose(A) if AT is None else AT
+        DT = csr_transpose(D)
         self.n = A[3]
         arrs = [np.ascontiguousarray(a, np.float32) for a in (max_dose, max_weights, min_dose, min_weights,
                                                                oar_weights)]

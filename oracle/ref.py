@@ -196,14 +196,17 @@ class OptProblem:
     them: MatCSR64 with 64-bit indices for A, Aᵀ, D, Dᵀ (Aᵀ and Dᵀ formed here
     as IMRTEigenLoad's transposes do)."""
 
-    def __init__(self, A, D, n_ptv, n_oar, max_dose, max_weights, min_dose, min_weights, oar_weights, gamma, eta):
+    def __init__(self, A, D, n_ptv, n_oar, max_dose, max_weights, min_dose, min_weights, oar_weights, gamma, eta,
+                 AT=None, DT=None):
         self.L = _opt_lib()
         self.keep = []
         self.n = int(A[3])
         arrs = [np.ascontiguousarray(a, np.float32) for a in (max_dose, max_weights, min_dose, min_weights,
                                                                oar_weights)]
         self.keep += arrs
-        cs = [_csr(m, self.keep) for m in (A, _transpose(A), D, _transpose(D))]
+        AT = _transpose(A) if AT is None else AT
+        DT = _transpose(D) if DT is None else DT
+        cs = [_csr(m, self.keep) for m in (A, AT, D, DT)]
         self.keep += cs
         self.h = self.L.ref_opt_problem_create(*(C.byref(c) for c in cs), n_ptv, n_oar, *(_p(a) for a in arrs),
                                                gamma, eta)

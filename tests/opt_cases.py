@@ -113,3 +113,42 @@ def prox_input(case):
     g0[bc[5]:bc[6]] = (seg / np.linalg.norm(seg) * np.sqrt(5e-5)).astype(np.float32)
     tau = rng.uniform(0.01, 1.0, len(counts)).astype(np.float32)
     return g0, tau
+
+
+def dim_reduction(active, counts, weights, x, v, nrm, n_keep):
+    """DimReduction (IMRTOptUtils.cu:726-793): keep the n_keep beams of largest
+    norm, strongest first, with their weights and fluence segments."""
+    offs = np.concatenate([[0], np.cumsum([counts[b] for b in active])]).astype(np.int64)
+    rank = sorted(range(len(active)), key=lambda j: -float(nrm[j]))[:n_keep]
+    keep = [active[j] for j in rank]
+    seg = lambda a: (np.concatenate([a[offs[j]:offs[j + 1]] for j in rank]).astype(np.float32)  # noqa: E731
+                     if rank else np.zeros(0, np.float32))
+    return keep, np.array([weights[j] for j in rank], np.float32), seg(x), seg(v)
+
+
+def oracle_outer(case, x0, beam_weights, prm=OUTER):
+    """BeamOrientationOptimization (IMRTOptimize.cu:197-388) over the oracle's
+    BOO: phases ended by the prune triggers, each followed by DimReduction."""
+    w = case["w"]
+    active = list(range(len(case["counts"])))
+    x = v = x0
+    weights = beam_weights
+    state = None
+    costs = np.zeros(prm["max_iter"], np.float32)
+    phases = []
+    while True:
+        A, D, _ = select(case, active)
+        O = oracle.Problem(A, D, case["n_ptv"], case["n_oar"], w["max_dose"], w["max_weights"], w["min_dose"],
+                           w["min_weights"], w["oar_weights"], case["gamma"], case["eta"])
+        go = np.concatenate([[0], np.cumsum([case["counts"][b] for b in active])]).astype(np.int64)
+        st = None if state is None else (state[0], state[1], state[2], v)
+        r = O.boo(go, weights, x, prm["step_size"], prm["max_iter"], prune=prm["prune"], want=prm["want"],
+                  change_trigger=prm["change_trigger"], state=st, loss=costs)
+        state = (r["k"], r["theta"], r["t"])
+        phases.append((list(active), r["k"], r["active"]))
+        active, weights, x, v = dim_reduction(active, case["counts"], r["weights"], r["x"], r["v"], r["nrm"],
+                                              int(r["active"]))
+        if r["stop"] or not active:
+            break
+    return dict(active=np.array(active, np.int32), x=x, v=v, weights=weights, costs=costs, state=state,
+                phases=phases)

@@ -207,3 +207,119 @@ def test_dose_c1_matches_reference(ctx):
     _gate(dose, g["dose_sum"].ravel())
     # row supports agree up to the point-sampling flips at the column edges
     assert np.abs(nnz - g["nnz"]).max() <= 0.02 * g["nnz"].max()
+
+
+# ------------------------------------------------------------------ the 4pi torso plan (config 2)
+# dose_c2_ref.npz: two beamlets from each of six oblique beams of the timed
+# 4pi plan, through the reference's Terma, CCCS and batched interpolation with
+# the 8x8 cone kernel (its 8x6 march never ends, see make_golden_dose.py).
+def _c2():
+    g = _gold("dose_c2_ref.npz")
+    cfg = phantoms.config2()
+    k88 = phantoms.synthetic_kernel(n_theta=8, n_phi=8)
+    np.testing.assert_array_equal(k88.phi, g["kernel_phi"])
+    from fastdose_b200.types import make_bundle
+
+    bund = make_bundle(cfg["isocenter"], cfg["angles"][0], sad=cfg["sad"], fluence_dim=cfg["fluence_dim"],
+                       beamlet_size=cfg["beamlet_size"], sub_fluence_dim=cfg["sub_fluence_dim"],
+                       sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+    return g, cfg, k88, oracle.beamlet_fluence(bund)
+
+
+def test_oracle_c2_terma_and_cccs_match_reference():
+    g, cfg, k88, fl = _c2()
+    ph = cfg["phantom"]
+    for j in (0, 6):
+        b = g["beams"][j]
+        T, R = oracle.terma(b, fl, ph.density, ph.volume, cfg["spectrum"], tex_mode=1)
+        ref = g[f"terma_{j}"]
+        assert np.abs(T.reshape(ref.shape) - ref).max() <= 2e-4 * ref.max()
+        D = oracle.cccs(b, T, R, k88).reshape(ref.shape)
+        ref = g[f"dose_{j}"]
+        sel = ref > 0.1 * ref.max()
+        assert np.abs(D - ref)[sel].mean() <= 1e-3 * ref.max()
+        assert np.abs(D - ref).max() <= 5e-2 * ref.max()  # the march's one-ulp sensitivity, see the module note
+
+
+def test_oracle_supersampled_bev2pvcs_matches_reference():
+    g = _gold("bev2pvcs_ss_ref.npz")
+    c = _gold("dose_c1_ref.npz")
+    vol = c1_case()["phantom"].volume
+    for ssf, ext in ((5, 2.0), (3, 0.6)):
+        ref = g[f"out_{ssf}"]
+        out = oracle.bev2pvcs_ss(g["beam"], c["dose_44"], vol, ssfactor=ssf, extent=ext, tex_mode=1).reshape(ref.shape)
+        assert np.abs(out - ref).max() <= 5e-3 * ref.max()
+        # voxels are written only inside the extent and above eps_fastdose: the
+        # written support differs only at that threshold
+        assert abs(int((out != 0).sum()) - int((ref != 0).sum())) <= max(4, (ref != 0).sum() // 1000)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("ssf,ext", [(5, 2.0), (3, 0.6)])
+def test_bev2pvcs_supersampling_matches_reference(ctx, ssf, ext):
+    """fd2_bev2pvcs_supersampling against fastdose::BEV2PVCS_SuperSampling
+    (FastDoseLib/src/geom.cu:343-474) on config-1 beamlet 44's dose."""
+    import torch
+
+    g = _gold("bev2pvcs_ss_ref.npz")
+    c = _gold("dose_c1_ref.npz")
+    case = c1_case()
+    dens = api.Density(ctx, case["phantom"].density, case["phantom"].volume)
+    out = api.BEV2PVCS(ctx, g["beam"], dens, torch.from_numpy(np.ascontiguousarray(c["dose_44"])).cuda(),
+                       ssfactor=ssf, extent=ext)
+    torch.cuda.synchronize()
+    out = out.cpu().numpy()
+    ref = g[f"out_{ssf}"]
+    # the reference interpolates through the texture unit (8-bit weights)
+    assert np.abs(out - ref).max() <= 5e-3 * ref.max()
+    assert abs(int((out != 0).sum()) - int((ref != 0).sum())) <= max(4, (ref != 0).sum() // 1000)
+
+
+@pytest.mark.gpu
+def test_c2_terma_and_cccs_match_reference(ctx):
+    """Six oblique beamlets of the 4pi torso plan: this library's Terma and CCCS
+    against the reference's BEV arrays, at the dose gate."""
+    import torch
+
+    g, cfg, k88, fl = _c2()
+    ph = cfg["phantom"]
+    idx = list(range(0, 12, 2))
+    batch = api.BEVBatch(g["beams"][idx])
+    dens = api.Density(ctx, ph.density, ph.volume)
+    api.TermaComputeCollective(ctx, batch, fl, dens, api.Spectrum(ctx, cfg["spectrum"]))
+    api.DoseComputeCollective(ctx, batch, api.Kernel(ctx, k88))
+    torch.cuda.synchronize()
+    for k, j in enumerate(idx):
+        T = batch.get("terma", k).cpu().numpy().reshape(g[f"terma_{j}"].shape)
+        assert np.abs(T - g[f"terma_{j}"]).max() <= 2e-3 * g[f"terma_{j}"].max()
+        D = batch.get("dose", k).cpu().numpy().reshape(g[f"dose_{j}"].shape)
+        _gate(D, g[f"dose_{j}"])
+
+
+@pytest.mark.gpu
+def test_c2_dose_columns_match_reference(ctx):
+    """The twelve sampled beamlets through DoseMatConstruction (Terma, CCCS,
+    columns): each dose column and their sum against the reference's."""
+    g, cfg, k88, fl = _c2()
+    ph = cfg["phantom"]
+    dens = api.Density(ctx, ph.density, ph.volume)
+    beams = [g["beams"][i:i + 2] for i in range(0, 12, 2)]
+    m = api.DoseMatConstruction(ctx, beams, fl, dens, api.Spectrum(ctx, cfg["spectrum"]), api.Kernel(ctx, k88))
+    ro, col, val = m.to_host()
+    nv = ph.density.size
+    total, total_ref = np.zeros(nv), np.zeros(nv)
+    worst = 0.0
+    for r in range(12):
+        row = np.zeros(nv, np.float64)
+        row[col[ro[r]:ro[r + 1]]] = val[ro[r]:ro[r + 1]]
+        ref = np.zeros(nv, np.float64)
+        ref[g[f"col_{r}"]] = g[f"val_{r}"]
+        total += row
+        total_ref += ref
+        worst = max(worst, np.abs(row - ref).max() / ref.max())
+        sel = ref > 0.1 * ref.max()
+        assert np.abs(row - ref)[sel].mean() <= MEAN_GATE * ref.max()
+        # the support: the point-sampled 5^3 average flips samples at the column's edges
+        assert abs(int(ro[r + 1] - ro[r]) - len(g[f"col_{r}"])) <= 0.02 * len(g[f"col_{r}"])
+    assert worst <= 2e-2, f"worst single-column max difference {worst:.3g} of that column's max"
+    _gate(total, total_ref)
