@@ -651,7 +651,7 @@ def _lat_stats(lat_s):
 
 
 def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_per_rate=20.0, seed=11, workers=2,
-               plain_requests=30):
+               plain_requests=30, graph_off_rate=10.0):
     """p50/p99 plan latency (arrival -> dose-loading matrix on the device) and
     beamlets/s of the service under Poisson arrivals at each rate, over
     min(n_requests, max(30, rate * seconds_per_rate)) requests (seconds_per_rate
@@ -659,7 +659,9 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
     time, one beam per construction call -- run live at 1 request/s over the
     first plain_requests requests.  At higher rates the plain single server is
     overloaded (its utilisation, rate x mean service time, is reported); its
-    latencies there are a FIFO replay of the service times measured live."""
+    latencies there are a FIFO replay of the service times measured live.
+    The service launches each construction batch as one CUDA graph; at
+    graph_off_rate the same arrivals also run with kernel-by-kernel launches."""
     import threading
 
     import torch
@@ -716,10 +718,13 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
             warmed.add(int(s["worker"]))
         if len(warmed) == workers:
             break
-    for lam in rates:
-        n = len(reqs) if seconds_per_rate <= 0 else min(len(reqs), max(30, int(lam * seconds_per_rate)))
+    arrivals = {}
+
+    def run_rate(lam, n, graph):
         sub = reqs[:n]
-        arr = np.cumsum(rng.exponential(1.0 / lam, size=n))
+        if lam not in arrivals:
+            arrivals[lam] = np.cumsum(rng.exponential(1.0 / lam, size=n))
+        arr = arrivals[lam]
         tickets = [None] * n
         t_base = svc.clock_ms()
 
@@ -728,7 +733,7 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
                 delay = t_base + 1e3 * a - svc.clock_ms()
                 if delay > 0:
                     time.sleep(delay * 1e-3)
-                tickets[i] = svc.submit(r["phantom"], r["beams"], r["fluence"], spec, kern)
+                tickets[i] = svc.submit(r["phantom"], r["beams"], r["fluence"], spec, kern, graph=graph)
 
         with ClockSampler(torch.cuda.current_device()) as clk:
             th = threading.Thread(target=submitter)
@@ -741,23 +746,26 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
                 stats.append(s)
         lat = np.array([s["end_ms"] - s["submit_ms"] for s in stats]) * 1e-3
         span_s = (max(s["end_ms"] for s in stats) - min(s["submit_ms"] for s in stats)) * 1e-3
+        return arr, dict(_lat_stats(lat), beamlets_per_s=sum(n_bl[:n]) / span_s, workers=workers, graph=graph,
+                         queue_p50_ms=float(np.percentile([s["start_ms"] - s["submit_ms"] for s in stats], 50)),
+                         # per request (arrival order): beamlets, worker, submit ms (from the first
+                         # submit), queue ms, run ms
+                         timeline=[[int(s["beamlets"]), int(s["worker"]), round(s["submit_ms"] - stats[0]["submit_ms"], 1),
+                                    round(s["start_ms"] - s["submit_ms"], 1), round(s["end_ms"] - s["start_ms"], 1)]
+                                   for s in stats],
+                         clocks=clk.summary())
+
+    for lam in rates:
+        n = len(reqs) if seconds_per_rate <= 0 else min(len(reqs), max(30, int(lam * seconds_per_rate)))
+        arr, svc_stats = run_rate(lam, n, graph=True)
         # the plain single server at this rate: FIFO replay of the live service times
         end, rl = 0.0, []
-        arr_p = arr[:n_plain]
-        for a, sv in zip(arr_p, service_s):
+        for a, sv in zip(arr[:n_plain], service_s):
             end = max(end, a) + sv
             rl.append(end - a)
         key = f"rate_{lam:g}_per_s"
         out[key] = {
-            "service": dict(_lat_stats(lat), beamlets_per_s=sum(n_bl[:n]) / span_s, workers=workers,
-                            queue_p50_ms=float(np.percentile([s["start_ms"] - s["submit_ms"] for s in stats], 50)),
-                            # per request (arrival order): beamlets, worker, submit ms (from the first
-                            # submit), queue ms, run ms
-                            timeline=[[int(s["beamlets"]), int(s["worker"]),
-                                       round(s["submit_ms"] - stats[0]["submit_ms"], 1),
-                                       round(s["start_ms"] - s["submit_ms"], 1), round(s["end_ms"] - s["start_ms"], 1)]
-                                      for s in stats],
-                            clocks=clk.summary()),
+            "service": svc_stats,
             "plain_single_beam": dict(_lat_stats(rl), utilisation=lam * mean_s,
                                       basis="live" if lam == 1.0 else
                                       f"FIFO replay of the {n_plain} live service times at this rate"),
@@ -765,6 +773,11 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
         if lam == 1.0:
             out[key]["plain_single_beam"].update({k: plain_live[k] for k in ("p50_ms", "p99_ms", "max_ms")},
                                                  basis="live")
+    if graph_off_rate:
+        n = min(len(reqs), max(30, int(graph_off_rate * seconds_per_rate))) if seconds_per_rate > 0 else len(reqs)
+        _, off = run_rate(graph_off_rate, n, graph=False)  # the same arrivals, kernel-by-kernel launches
+        off.pop("timeline")
+        out[f"rate_{graph_off_rate:g}_per_s"]["service_without_graphs"] = off
     svc.close()
     return out
 

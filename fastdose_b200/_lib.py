@@ -77,6 +77,7 @@ _PROTOS = {
     "fd2_dvh": (_i, [_vp, _vp, _i64, _i64, _vp, _vp, _i, _f, _vp, _vp]),
     "fd2_csr_ensemble_concat": (_i, [_vp, _sz, _vp, _vp]),
     "fd2_context_tuned_schedules": (_i, [_vp, _sz, _vp, _vp, _vp, _vp]),
+    "fd2_context_graph_counts": (_i, [_vp, _vp, _vp, _vp]),
     "fd2_opt_problem_set_graph": (_i, [_vp, _i]),
     "fd2_opt_problem_set_reducer": (_i, [_vp, _vp, _vp]),
     "fd2_bundles_beamlets": (_i, [_sz, _vp, _vp, _vp, _i, _sz, _vp, _vp]),

@@ -126,6 +126,13 @@ class Context:
     def launch_count(self):
         return int(self.lib.fd2_context_launch_count(self.h))
 
+    def graph_counts(self):
+        """Graph-captured construction: (batches launched as graphs, executable
+        graphs instantiated, in-place updates)."""
+        v = [C.c_uint64(0) for _ in range(3)]
+        _lib.check(self.lib.fd2_context_graph_counts(self.h, *(C.byref(x) for x in v)), "graph_counts")
+        return tuple(int(x.value) for x in v)
+
     def close(self):
         if self.h:
             self.lib.fd2_context_destroy(self.h)
@@ -332,7 +339,7 @@ def beamletFlagInit(ctx, bundles, ptv_mask, volume, super_sampling=3):
 class _Params(C.Structure):
     _fields_ = [("extent", C.c_float), ("ss_factor", C.c_int), ("value_type", C.c_int), ("cccs_schedule", C.c_int),
                 ("batch_beamlets", C.c_uint64), ("memory_budget", C.c_uint64), ("verbose", C.c_int),
-                ("host_out", C.c_void_p)]
+                ("host_out", C.c_void_p), ("graph", C.c_int)]
 
 
 class _HostCSR(C.Structure):
@@ -455,11 +462,12 @@ class MatCSREnsemble:
 
 def DoseMatConstruction(ctx, beamlets_per_beam, fluence, density, spectrum, kernel, extent=2.0, ss_factor=5,
                         value_type="f32", cccs_schedule=-1, memory_budget=0, batch_beamlets=0, verbose=False,
-                        stream=None, host_out=None):
+                        stream=None, host_out=None, graph=False):
     """IMRT::DoseMatConstruction: `beamlets_per_beam` is a list of BEAM_DTYPE
     arrays (one per beam).  Returns a MatCSREnsemble.  host_out: a HostCSR
     (of this value type) that receives a host copy of the matrix, batch by
-    batch while it is built."""
+    batch while it is built.  graph: each batch launched as one CUDA graph
+    (kept per batch shape in the context and updated in place)."""
     counts = np.array([len(b) for b in beamlets_per_beam], np.uint32)
     allb = np.ascontiguousarray(np.concatenate([np.asarray(b, BEAM_DTYPE).reshape(-1) for b in beamlets_per_beam]),
                                 BEAM_DTYPE) if len(beamlets_per_beam) else np.zeros(0, BEAM_DTYPE)
@@ -472,7 +480,7 @@ def DoseMatConstruction(ctx, beamlets_per_beam, fluence, density, spectrum, kern
             raise ValueError(f"host_out holds {host_out.row_off.numel() - 1} rows, the plan has {allb.size}")
         hs = host_out._struct()
     prm = _Params(extent, ss_factor, VALUE_TYPES[value_type], cccs_schedule, batch_beamlets, memory_budget,
-                  int(verbose), C.cast(C.pointer(hs), C.c_void_p) if hs is not None else None)
+                  int(verbose), C.cast(C.pointer(hs), C.c_void_p) if hs is not None else None, int(bool(graph)))
     h = C.c_void_p()
     st = ctx.lib.fd2_dose_mat_construct(ctx.h, len(counts), _p(counts), _p(allb), _p(fl), density.h, spectrum.h,
                                         kernel.h, C.byref(prm), C.byref(h),

@@ -671,6 +671,20 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     return FD2_OK;
 }
 
+size_t cccs_scratch_bytes(size_t n_beams, const fd2_beam_t* h_beams, const fd2_cccs_kernel* k, int schedule) {
+    size_t n_fwd = 0;
+    for (int t = 0; t < k->n_theta; t++)
+        if ((double)k->theta[t] <= 1.5707963267948966) n_fwd++;
+    size_t maxP = 0, maxL = 0;
+    for (size_t i = 0; i < n_beams; i++) {
+        maxP = std::max(maxP, (size_t)h_beams[i].fmap_size[0] * h_beams[i].fmap_size[1]);
+        maxL = std::max(maxL, (size_t)h_beams[i].long_dim);
+    }
+    const size_t dir_bytes = n_beams * n_fwd * k->n_phi * sizeof(float4);
+    const size_t plane_bytes = schedule == 1 ? n_beams * n_fwd * maxP * maxL * sizeof(float) : 0;
+    return dir_bytes + plane_bytes + 256;
+}
+
 // Automatic schedule: split the zenith bins across blocks when the beamlets
 // alone cannot fill the device (fewer than ~4 blocks per SM).
 int cccs_auto_schedule(const fd2_context* ctx, size_t n_beams) {

@@ -25,6 +25,21 @@ int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, cudaStream_t st, void**
     return FD2_OK;
 }
 
+void ctx_graphs_free(fd2_context* ctx) {
+    for (auto& kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+    ctx->graphs.clear();
+    for (int i = 0; i < 2; i++) {
+        if (ctx->stage_free[i]) {
+            cudaEventSynchronize(ctx->stage_free[i]);
+            cudaEventDestroy(ctx->stage_free[i]);
+        }
+        if (ctx->h_stage[i]) cudaFreeHost(ctx->h_stage[i]);
+        ctx->stage_free[i] = nullptr;
+        ctx->h_stage[i] = nullptr;
+        ctx->h_stage_bytes[i] = 0;
+    }
+}
+
 int density_create_pooled(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume,
                           fd2_density** out) {
     FD2_REQUIRE(ctx && host_density && volume && out, FD2_ERR_INVALID_ARGUMENT, "density_create: null argument");
@@ -94,6 +109,7 @@ int fd2_context_destroy(fd2_context* c) {
     if (!c) return FD2_OK;
     cudaSetDevice(c->device);
     cudaDeviceSynchronize();  // no work of any stream still uses the context's memory
+    fd2::ctx_graphs_free(c);
     for (void* b : c->buf)
         if (b) cudaFreeAsync(b, c->stream);
     if (c->d_status) cudaFree(c->d_status);
@@ -112,6 +128,7 @@ int fd2_context_destroy(fd2_context* c) {
 int fd2_context_release(fd2_context* c) {
     FD2_REQUIRE(c, FD2_ERR_INVALID_ARGUMENT, "null context");
     FD2_CHECK_CUDA(cudaDeviceSynchronize());  // no work of any stream still uses the buffers
+    fd2::ctx_graphs_free(c);  // the graphs name the buffers freed below
     for (int i = 0; i < fd2::kBufCount; i++) {
         if (c->buf[i]) FD2_CHECK_CUDA(cudaFreeAsync(c->buf[i], c->stream));
         c->buf[i] = nullptr;
@@ -120,6 +137,14 @@ int fd2_context_release(fd2_context* c) {
     }
     FD2_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     FD2_CHECK_CUDA(cudaMemPoolTrimTo(c->pool, 0));
+    return FD2_OK;
+}
+
+int fd2_context_graph_counts(fd2_context* c, uint64_t* launches, uint64_t* instantiations, uint64_t* updates) {
+    FD2_REQUIRE(c, FD2_ERR_INVALID_ARGUMENT, "null context");
+    if (launches) *launches = c->graph_launches;
+    if (instantiations) *instantiations = c->graph_instantiations;
+    if (updates) *updates = c->graph_updates;
     return FD2_OK;
 }
 

@@ -250,8 +250,20 @@ static int ensemble_sync_nnz(fd2_csr_ensemble* e) {
 // scales by a device scan, then the rows gathered into the ensemble -- all in
 // stream order, without waiting for the device (the exact nonzero count is
 // read when the matrix is complete, or when the capacity bound runs out).
+// Scratch of one batch's column stage: the candidate offsets (already on the
+// device), row nonzero counts, row maxima and inverse row scales.  Direct
+// launches take them from the pool; a graph-captured batch passes them in
+// the context's batch buffer, since nothing may be allocated under capture.
+struct ColumnScratch {
+    uint64_t* cap_off = nullptr;
+    uint32_t* nnz = nullptr;
+    float* max = nullptr;
+    float* iscale = nullptr;
+};
+
 static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const uint32_t* cnt, size_t nb,
-                          const float* const* aD, const fd2_volume_t& vol, float extent, int ss, cudaStream_t st) {
+                          const float* const* aD, const fd2_volume_t& vol, float extent, int ss, cudaStream_t st,
+                          const ColumnScratch* pre = nullptr) {
     fd2_context* ctx = e->ctx;
     uint32_t* d_nnz = nullptr;
     uint64_t* d_cap_off = nullptr;
@@ -259,21 +271,34 @@ static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const 
     int rc = [&]() -> int {
         std::vector<uint64_t> cap(nb + 1, 0);
         for (size_t k = 0; k < nb; k++) cap[k + 1] = cap[k] + cnt[k];
-        if (e->nnz_bound + cap[nb] > e->nnz_cap) {  // the bound may not fit: use the exact count
-            FD2_TRY(ensemble_sync_nnz(e));
-            FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz + cap[nb]));
+        if (pre) {
+            // the construction reserved every beamlet's candidates up front
+            FD2_REQUIRE(e->nnz_bound + cap[nb] <= e->nnz_cap && e->n_rows + nb + 1 <= e->row_cap, FD2_ERR_CAPACITY,
+                        "dose_mat_construct: graph batch beyond the reserved matrix");
+        } else {
+            if (e->nnz_bound + cap[nb] > e->nnz_cap) {  // the bound may not fit: use the exact count
+                FD2_TRY(ensemble_sync_nnz(e));
+                FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz + cap[nb]));
+            }
+            FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz_bound + cap[nb]));
         }
-        FD2_TRY(ensemble_reserve(e, e->n_rows + nb, e->nnz_bound + cap[nb]));
         const uint64_t ncap = std::max<uint64_t>(1, cap[nb]);
         void* tmp = nullptr;
         FD2_TRY(ctx_buffer(ctx, kBufColumns, ncap * (sizeof(int32_t) + sizeof(float)), st, &tmp));
         int32_t* d_tcol = (int32_t*)tmp;
         float* d_tval = (float*)(d_tcol + ncap);
-        FD2_TRY(upload(cap, &d_cap_off, ctx->pool, st));
-        FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_nnz, nb * sizeof(uint32_t), ctx->pool, st));
-        FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_max, nb * sizeof(float), ctx->pool, st));
         const bool half = e->value_type != FD2_VALUES_F32;
-        if (half) FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_iscale, nb * sizeof(float), ctx->pool, st));
+        if (pre) {
+            d_cap_off = pre->cap_off;
+            d_nnz = pre->nnz;
+            d_max = pre->max;
+            d_iscale = half ? pre->iscale : nullptr;
+        } else {
+            FD2_TRY(upload(cap, &d_cap_off, ctx->pool, st));
+            FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_nnz, nb * sizeof(uint32_t), ctx->pool, st));
+            FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_max, nb * sizeof(float), ctx->pool, st));
+            if (half) FD2_CHECK_CUDA(cudaMallocFromPoolAsync((void**)&d_iscale, nb * sizeof(float), ctx->pool, st));
+        }
         FD2_TRY(launch_column_values(d_infos, nb, aD, d_cap_off, d_tcol, d_tval, d_nnz, d_max, vol, extent, ss, st));
         int64_t* d_roff = e->d_row_off + e->n_rows;  // [0] is this batch's first offset
         FD2_TRY(launch_column_rows(nb, d_nnz, d_max, d_roff, half ? e->d_scale + e->n_rows : nullptr, d_iscale, st));
@@ -286,9 +311,120 @@ static int append_columns(fd2_csr_ensemble* e, const ColumnInfo* d_infos, const 
             std::printf("  columns: %zu beamlets, %llu candidates enqueued\n", nb, (unsigned long long)cap[nb]);
         return FD2_OK;
     }();
-    for (void* p : {(void*)d_nnz, (void*)d_cap_off, (void*)d_max, (void*)d_iscale})
-        if (p) cudaFreeAsync(p, st);
+    if (!pre)
+        for (void* p : {(void*)d_nnz, (void*)d_cap_off, (void*)d_max, (void*)d_iscale})
+            if (p) cudaFreeAsync(p, st);
     return rc;
+}
+
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// One batch of the construction captured as a CUDA graph and launched with
+// one call (fd2_dosemat_params_t.graph).  Everything the batch touches is
+// sized before the capture -- the BEV, column, cone and batch buffers of the
+// context, and the pinned staging of its small tables -- so the capture holds
+// only copies, memsets and kernels.  The context keeps one executable graph
+// per batch shape; a later batch of that shape updates it in place
+// (cudaGraphExecUpdate: new pointers, sizes and grid extents) and a refused
+// update instantiates afresh.  The kernels, their order and their inputs are
+// those of the direct path, so the matrix is the same bit for bit.
+static int graph_batch(fd2_context* ctx, fd2_csr_ensemble* e, size_t nb, const fd2_beam_t* h_beams,
+                       const fd2_beam_t* d_beams, const ColumnInfo* d_infos, const uint32_t* cnt,
+                       const float* d_fluence, float* dT, float* dR, float* dD, const size_t* off, size_t P,
+                       const fd2_density* density, const fd2_spectrum* spectrum, const fd2_cccs_kernel* kernel,
+                       const fd2_dosemat_params_t& params, int schedule, cudaStream_t st) {
+    // device layout of the batch buffer: aF, aT, aR, aD (pointers), candidate
+    // offsets -- uploaded from the staging -- then the column-stage scratch
+    const size_t up_bytes = (4 * nb + nb + 1) * sizeof(uint64_t);
+    const size_t o_nnz = align256(up_bytes), o_max = o_nnz + align256(nb * 4), o_isc = o_max + align256(nb * 4);
+    const size_t dev_bytes = o_isc + align256(nb * 4);
+    uint64_t ncap_total = 0;
+    for (size_t k = 0; k < nb; k++) ncap_total += cnt[k];
+    void *batch = nullptr, *scratch = nullptr, *cols = nullptr;
+    FD2_TRY(ctx_buffer(ctx, kBufBatch, dev_bytes, st, &batch));
+    FD2_TRY(ctx_scratch(ctx, cccs_scratch_bytes(nb, h_beams, kernel, schedule), st, &scratch));
+    FD2_TRY(ctx_buffer(ctx, kBufColumns, std::max<uint64_t>(1, ncap_total) * (sizeof(int32_t) + sizeof(float)), st,
+                       &cols));
+    // pinned staging: a slot is refilled once the graph that read it has run
+    const int slot = ctx->stage_slot;
+    ctx->stage_slot ^= 1;
+    if (ctx->stage_free[slot]) FD2_CHECK_CUDA(cudaEventSynchronize(ctx->stage_free[slot]));
+    else FD2_CHECK_CUDA(cudaEventCreateWithFlags(&ctx->stage_free[slot], cudaEventDisableTiming));
+    if (ctx->h_stage_bytes[slot] < up_bytes) {
+        if (ctx->h_stage[slot]) FD2_CHECK_CUDA(cudaFreeHost(ctx->h_stage[slot]));
+        ctx->h_stage[slot] = nullptr;
+        ctx->h_stage_bytes[slot] = 0;
+        FD2_CHECK_CUDA(cudaHostAlloc(&ctx->h_stage[slot], up_bytes, cudaHostAllocDefault));
+        ctx->h_stage_bytes[slot] = up_bytes;
+    }
+    uint64_t* h = (uint64_t*)ctx->h_stage[slot];
+    for (size_t k = 0; k < nb; k++) {
+        h[k] = (uint64_t)(uintptr_t)d_fluence;
+        h[nb + k] = (uint64_t)(uintptr_t)(dT + off[k]);
+        h[2 * nb + k] = (uint64_t)(uintptr_t)(dR + off[k]);
+        h[3 * nb + k] = (uint64_t)(uintptr_t)(dD + off[k]);
+    }
+    uint64_t* hc = h + 4 * nb;
+    hc[0] = 0;
+    for (size_t k = 0; k < nb; k++) hc[k + 1] = hc[k] + cnt[k];
+    char* b = (char*)batch;
+    const float** aF = (const float**)b;
+    float** aT = (float**)(b + nb * 8);
+    float** aR = (float**)(b + 2 * nb * 8);
+    float** aD = (float**)(b + 3 * nb * 8);
+    ColumnScratch pre;
+    pre.cap_off = (uint64_t*)(b + 4 * nb * 8);
+    pre.nnz = (uint32_t*)(b + o_nnz);
+    pre.max = (float*)(b + o_max);
+    pre.iscale = (float*)(b + o_isc);
+
+    FD2_CHECK_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    int rc = [&]() -> int {
+        FD2_CHECK_CUDA(cudaMemcpyAsync(batch, h, up_bytes, cudaMemcpyHostToDevice, st));
+        FD2_CHECK_CUDA(cudaMemsetAsync(dD, 0, off[nb] * sizeof(float), st));
+        FD2_TRY(launch_terma(ctx, P, nb, d_beams, aF, aT, aR, density, spectrum, 1, st));
+        FD2_TRY(launch_cccs_host(ctx, nb, h_beams, d_beams, (const float* const*)aT, (const float* const*)aR, aD,
+                                 kernel, schedule, st));
+        return append_columns(e, d_infos, cnt, nb, (const float* const*)aD, density->vol, params.extent,
+                              params.ss_factor, st, &pre);
+    }();
+    cudaGraph_t g = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);  // the capture ends on every path
+    if (rc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        if (rc) return rc;
+        FD2_CHECK_CUDA(ce);
+    }
+    const uint64_t key = (uint64_t)h_beams[0].fmap_size[0] | (uint64_t)h_beams[0].fmap_size[1] << 10 |
+                         (uint64_t)kernel->n_phi << 20 | (uint64_t)kernel->n_theta << 28 | (uint64_t)schedule << 36 |
+                         (uint64_t)params.value_type << 38 | (uint64_t)params.ss_factor << 40;
+    cudaGraphExec_t ex = nullptr;
+    auto it = ctx->graphs.find(key);
+    if (it != ctx->graphs.end()) {
+        cudaGraphExecUpdateResultInfo info;
+        if (cudaGraphExecUpdate(it->second, g, &info) == cudaSuccess) {
+            ex = it->second;
+            ctx->graph_updates++;
+        } else {
+            cudaGetLastError();  // a refused update is not an error: instantiate afresh
+            cudaGraphExecDestroy(it->second);
+            ctx->graphs.erase(it);
+        }
+    }
+    cudaError_t err = cudaSuccess;
+    if (!ex) {
+        err = cudaGraphInstantiate(&ex, g, 0);
+        if (err == cudaSuccess) {
+            ctx->graphs[key] = ex;
+            ctx->graph_instantiations++;
+        }
+    }
+    cudaGraphDestroy(g);
+    FD2_CHECK_CUDA(err);
+    FD2_CHECK_CUDA(cudaGraphLaunch(ex, st));
+    ctx->graph_launches++;
+    FD2_CHECK_CUDA(cudaEventRecord(ctx->stage_free[slot], st));
+    return FD2_OK;
 }
 
 // The host copy of a matrix under construction (fd2_dosemat_params_t.host_out).
@@ -395,6 +531,7 @@ void fd2_dosemat_params_default(fd2_dosemat_params_t* p) {
     p->memory_budget = 0;
     p->verbose = 0;
     p->host_out = nullptr;
+    p->graph = 0;
 }
 
 int fd2_bev2pvcs(fd2_context* ctx, const fd2_beam_t* h_beam, const fd2_density* density, const float* d_bev,
@@ -435,6 +572,9 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     FD2_REQUIRE(params.value_type >= 0 && params.value_type <= 2, FD2_ERR_INVALID_ARGUMENT, "bad value type");
     FD2_REQUIRE(params.cccs_schedule >= -2 && params.cccs_schedule <= 1, FD2_ERR_INVALID_ARGUMENT,
                 "cccs_schedule %d (-2..1)", params.cccs_schedule);
+    FD2_REQUIRE(params.graph == 0 || params.graph == 1, FD2_ERR_INVALID_ARGUMENT, "graph %d (0 or 1)", params.graph);
+    FD2_REQUIRE(!(params.graph && params.host_out), FD2_ERR_NOT_SUPPORTED,
+                "dose_mat_construct: graph capture and host_out are exclusive");
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
     const fd2_volume_t& vol = density->vol;
     const uint64_t nvox = (uint64_t)vol.dim[0] * vol.dim[1] * vol.dim[2];
@@ -523,6 +663,20 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         rc = ctx_buffer(ctx, kBufBev, off[nb] * 3 * sizeof(float), st, (void**)&d_bev);
         if (rc) break;
         float *dT = d_bev, *dR = d_bev + off[nb], *dD = d_bev + 2 * off[nb];
+        if (params.graph) {
+            const int sched = params.cccs_schedule >= 0 ? params.cccs_schedule : cccs_auto_schedule(ctx, nb);
+            rc = graph_batch(ctx, e, nb, beams.data() + b0, d_beams + b0, d_infos + b0, cnt.data() + b0, d_fluence,
+                             dT, dR, dD, off.data(), P, density, spectrum, kernel, params, sched, st);
+            if (rc) break;
+            size_t row = e->n_rows - nb;
+            for (size_t i = beam0; i < beam1; i++) {
+                row += n_per_beam[i];
+                e->mat_rows.push_back(row);
+            }
+            b0 = b1;
+            beam0 = beam1;
+            continue;
+        }
         std::vector<const float*> hF(nb, d_fluence);
         std::vector<float*> hT(nb), hR(nb), hD(nb);
         for (size_t k = 0; k < nb; k++) { hT[k] = dT + off[k]; hR[k] = dR + off[k]; hD[k] = dD + off[k]; }

@@ -75,6 +75,16 @@ struct fd2_context {
     // autotuned CCCS schedule (0 or 1) per batch shape, measured on first use
     std::unordered_map<uint64_t, int> cccs_schedule;
     uint64_t tuning_runs = 0;  // batches on which both schedules were timed
+    // graph-captured construction (fd2_dosemat_params_t.graph): one executable
+    // graph per batch shape, updated in place for each batch; the batch's small
+    // tables go up from pinned staging (two slots, each reused once the graph
+    // that read it has run)
+    std::unordered_map<uint64_t, cudaGraphExec_t> graphs;
+    void* h_stage[2] = {nullptr, nullptr};
+    size_t h_stage_bytes[2] = {0, 0};
+    cudaEvent_t stage_free[2] = {nullptr, nullptr};
+    int stage_slot = 0;
+    uint64_t graph_launches = 0, graph_instantiations = 0, graph_updates = 0;
 };
 
 namespace fd2 {
@@ -137,7 +147,7 @@ namespace fd2 {
 // (calls on one context are serialised: one host thread, work in stream
 // order); growing it replaces the old one in the order of stream `st`, and
 // waits for the device only when the previous use was on another stream.
-enum CtxBuffer { kBufCccs = 0, kBufBev = 1, kBufColumns = 2, kBufCount = 4 };
+enum CtxBuffer { kBufCccs = 0, kBufBev = 1, kBufColumns = 2, kBufBatch = 3, kBufCount = 4 };
 int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, cudaStream_t st, void** out);
 inline int ctx_scratch(fd2_context* ctx, size_t bytes, cudaStream_t st, void** out) {
     return ctx_buffer(ctx, kBufCccs, bytes, st, out);
@@ -179,6 +189,14 @@ struct ConeAngles {
 // Device table of cone directions, float4 [beam][theta_fwd][phi] (cccs_dirs.cu).
 int launch_cone_dirs(const fd2_beam_t* d_beams, size_t n_beams, const ConeAngles& ang, float4* d_out,
                      cudaStream_t stream);
+
+// Bytes of context scratch launch_cccs_host needs for a batch (the direction
+// table, and the per-zenith planes of schedule 1), so a caller can size the
+// scratch before a stream capture.
+size_t cccs_scratch_bytes(size_t n_beams, const fd2_beam_t* h_beams, const fd2_cccs_kernel* k, int schedule);
+
+// Graph state of a context: executable graphs, pinned staging, events.
+void ctx_graphs_free(fd2_context* ctx);
 
 // Launchers used by the plan-level code (dosemat.cu).
 int launch_terma(fd2_context* ctx, size_t fmap_npixels, size_t n_beams, const fd2_beam_t* d_beams,

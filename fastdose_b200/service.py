@@ -61,8 +61,10 @@ class Service:
         return self.lib.fd2_service_clock_ms(self.h)
 
     def submit(self, phantom, beamlets_per_beam, fluence, spectrum, kernel, extent=2.0, ss_factor=5,
-               value_type="f32"):
-        """Queues one plan; returns its ticket.  The inputs are copied."""
+               value_type="f32", graph=False):
+        """Queues one plan; returns its ticket.  The inputs are copied.  graph:
+        the worker launches each construction batch as one CUDA graph (kept
+        per batch shape on the worker's context and updated in place)."""
         keep = []
 
         def arr(x, dt):
@@ -82,7 +84,7 @@ class Service:
                     (C.c_uint32 * 3)(*vol["bbox_start"]), (C.c_uint32 * 3)(*vol["bbox_dim"]))
         req = _Request(_p(dens), v, len(counts), _p(counts), _p(allb), _p(fl), spectrum.n, *(_p(x) for x in sp),
                        kernel.n_theta, *(_p(x) for x in kn), kernel.n_phi, _p(phi),
-                       _Params(extent, ss_factor, VALUE_TYPES[value_type], -1, 0, 0, 0, None))
+                       _Params(extent, ss_factor, VALUE_TYPES[value_type], -1, 0, 0, 0, None, int(bool(graph))))
         t = C.c_uint64()
         _lib.check(self.lib.fd2_service_submit(self.h, C.byref(req), C.byref(t)), "service_submit")
         return t.value

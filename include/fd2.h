@@ -178,6 +178,14 @@ uint64_t fd2_context_launch_count(const fd2_context* ctx);
  */
 int fd2_context_tuned_schedules(const fd2_context* ctx, size_t cap, uint64_t* keys, int32_t* schedules, size_t* n,
                                 uint64_t* runs);
+/*
+ * Graph-captured construction (fd2_dosemat_params_t.graph) on this context:
+ * batches launched as one graph, executable graphs instantiated (one per
+ * batch shape, or again when an in-place update is refused), and in-place
+ * updates.  The reference has no counterpart (it launches kernel by kernel).
+ * Any pointer may be NULL.
+ */
+int fd2_context_graph_counts(fd2_context* ctx, uint64_t* launches, uint64_t* instantiations, uint64_t* updates);
 
 /*
  * fastdose::density_h2d (FastDoseLib/src/density.cu:23-58).  Copies a host

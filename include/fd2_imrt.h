@@ -67,6 +67,15 @@ typedef struct fd2_dosemat_params {
     int verbose;                /* print per-batch timings to stdout */
     fd2_host_csr_t* host_out;   /* NULL (default), or host buffers the matrix is copied into
                                    batch by batch as it is built (fd2_dose_mat_construct only) */
+    int graph;                  /* 0 (default): each batch's work is launched call by call.
+                                   1: each batch's device work -- uploads of its descriptor tables,
+                                   Terma, cone directions, CCCS, column values, row offsets, gather
+                                   -- is captured as one CUDA graph and launched with one call; the
+                                   context keeps one executable graph per batch shape (map size,
+                                   cones, schedule, value type, supersampling) and updates it in
+                                   place with the next batch's parameters.  The CCCS schedule is
+                                   then fixed per batch (-1 acts as -2), and the matrix is bit for
+                                   bit the one direct launches give.  fd2_dose_mat_construct only. */
 } fd2_dosemat_params_t;
 
 void fd2_dosemat_params_default(fd2_dosemat_params_t* p);

@@ -148,6 +148,49 @@ def test_tuned_cccs_schedule(ctx):
     c2.close()
 
 
+@pytest.mark.parametrize("vt,sched", [("f32", 0), ("f16", 1), ("f32", -1)])
+def test_graph_captured_construction_matches_direct(vt, sched):
+    """Batches launched as captured CUDA graphs give the matrix of direct
+    launches bit for bit, over several batches of one shape (the executable
+    graph is instantiated once and updated in place for the others) and over
+    a second plan on the same context."""
+    from fastdose_b200 import api as _api
+
+    c2 = _api.Context(0)
+    case = c1_case()
+    dens, sp, kn, _, _ = _setup(c2, case)
+    beams = [case["beams"][i:i + 10] for i in range(0, 100, 10)]  # 10 beams of 10 beamlets
+    fixed = -2 if sched < 0 else sched  # graph mode fixes the schedule per batch
+    ref = _api.DoseMatConstruction(c2, beams, case["fluence"], dens, sp, kn, value_type=vt, cccs_schedule=fixed,
+                                   batch_beamlets=30)
+    want = ref.to_host()
+    rows_want = ref.mat_rows()
+    for rep in range(2):
+        m = _api.DoseMatConstruction(c2, beams, case["fluence"], dens, sp, kn, value_type=vt, cccs_schedule=sched,
+                                     batch_beamlets=30, graph=True)
+        for a, b in zip(m.to_host(), want):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(m.mat_rows(), rows_want)
+        m.close()
+    launches, inst, updates = c2.graph_counts()
+    # four batches per plan (30, 30, 30, 10 beamlets), two plans
+    assert launches == 8 and inst >= 1 and inst + updates == 8
+    assert inst <= 2, f"{inst} instantiations: the in-place update was refused"
+    for h in (ref, dens, sp, kn):
+        h.close()
+    c2.close()
+
+
+def test_graph_construction_refuses_host_out(ctx):
+    from fastdose_b200 import _lib
+
+    case = small_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    host = api.HostCSR(len(case["beams"]), 10 ** 6)
+    with pytest.raises(_lib.FD2Error):
+        api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn, host_out=host, graph=True)
+
+
 def test_columns_match_oracle(ctx):
     case = small_case()
     beams, out, _, _ = _run_bev(ctx, case, list(range(16)))
