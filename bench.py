@@ -1054,7 +1054,8 @@ def run_fd2(args, rank, world):
         gc.collect()
         torch.cuda.empty_cache()
         ctx.release()
-        line["served"] = served_leg(ctx, n_requests=args.served_requests, seconds_per_rate=args.served_seconds,
+        line["served"] = served_leg(ctx, rates=tuple(float(r) for r in args.served_rates.split(",")),
+                                    n_requests=args.served_requests, seconds_per_rate=args.served_seconds,
                                     workers=args.served_workers)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, beamlets, fluence, args.cpu_seconds, os.cpu_count() or 1)[0]
@@ -1083,6 +1084,7 @@ def main():
     ap.add_argument("--served-seconds", type=float, default=20.0,
                     help="arrival seconds per rate (caps the requests at low rates); 0: all requests at every rate")
     ap.add_argument("--plain-requests", type=int, default=30, help="requests of the live plain-form run")
+    ap.add_argument("--served-rates", default="1,5,10,20,50", help="arrival rates (requests/s) of the served leg")
     ap.add_argument("--e2e-batch", type=int, default=-1,
                     help="beamlets per construction batch of the end-to-end leg (-1: a sixth of the plan, >= 4096)")
     ap.add_argument("--c4", action="store_true", help="run the multi-isocentre configuration alone")
@@ -1115,7 +1117,8 @@ def main():
         if args.only_optimizer:
             print(json.dumps({"optimizer": optimizer_leg(ctx, args.opt_iters, args.opt_rows)}), flush=True)
         else:
-            print(json.dumps({"served": served_leg(ctx, n_requests=args.served_requests,
+            print(json.dumps({"served": served_leg(ctx, rates=tuple(float(r) for r in args.served_rates.split(",")),
+                                                   n_requests=args.served_requests,
                                                    seconds_per_rate=args.served_seconds,
                                                    workers=args.served_workers, plain_requests=args.plain_requests)}),
                   flush=True)

@@ -170,12 +170,13 @@ __device__ __forceinline__ float exp2_sfu(float x) {
     return y;
 }
 
-// Segment length sqrt(l2) as l2 * rsqrt(l2) with the SFU reciprocal square
-// root (PTX rsqrt.approx.ftz.f32); l2 > 0 for every segment the march takes.
+// Segment length sqrt(l2) with the SFU square root (PTX sqrt.approx.ftz.f32),
+// the operation the reference's fast-math sqrtf becomes in d_calcLineSeg
+// (DoseComp.cu:143); l2 > 0 for every segment the march takes.
 __device__ __forceinline__ float seg_length(float l2) {
     float r;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l2));
-    return l2 * r;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l2));
+    return r;
 }
 
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
@@ -237,6 +238,7 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
     float2* tr = smem;
     float2* dp = smem + g.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const bool last_phi = warp == n_phi - 1;  // uniform per warp
     float2* mydp = dp + (size_t)warp * g.P;
     // kFx16: every azimuth warp keeps its own copy of the slice beside its sums,
     // wb[warp][v] = {Terma, density, dose, path sum}, so a ray step reads all
@@ -365,7 +367,12 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                         const float p = len * e.y;
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
-                        *reinterpret_cast<float2*>(&v->z) = make_float2(e.z + dep, e.w + p);
+                        // only the last azimuth's path sums are read (quirk Q2): the
+                        // other warps keep the dose alone
+                        if (last_phi)
+                            *reinterpret_cast<float2*>(&v->z) = make_float2(e.z + dep, e.w + p);
+                        else
+                            v->z = e.z + dep;
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - e.x, e.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - e.x, e.x);
                     };
@@ -399,10 +406,14 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                         if (on) {
-                            float2 acc = mydp[mi];
-                            acc.x += dep;
-                            acc.y += p;
-                            mydp[mi] = acc;
+                            if (last_phi) {
+                                float2 acc = mydp[mi];
+                                acc.x += dep;
+                                acc.y += p;
+                                mydp[mi] = acc;
+                            } else {
+                                mydp[mi].x += dep;
+                            }
                         }
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
@@ -444,10 +455,14 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                         if (on) {
                             float2* acc_p = reinterpret_cast<float2*>(reinterpret_cast<char*>(mydp) + mb);
-                            float2 acc = *acc_p;
-                            acc.x += dep;
-                            acc.y += p;
-                            *acc_p = acc;
+                            if (last_phi) {
+                                float2 acc = *acc_p;
+                                acc.x += dep;
+                                acc.y += p;
+                                *acc_p = acc;
+                            } else {
+                                acc_p->x += dep;
+                            }
                         }
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
@@ -471,10 +486,14 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                     const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                     const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                     if (act[j]) {
-                        float2 acc = mydp[mi];
-                        acc.x += dep;
-                        acc.y += p;
-                        mydp[mi] = acc;
+                        if (last_phi) {
+                            float2 acc = mydp[mi];
+                            acc.x += dep;
+                            acc.y += p;
+                            mydp[mi] = acc;
+                        } else {
+                            mydp[mi].x += dep;
+                        }
                     }
                     XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                     XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);

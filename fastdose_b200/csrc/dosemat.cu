@@ -351,11 +351,15 @@ static int graph_batch(fd2_context* ctx, fd2_csr_ensemble* e, size_t nb, const f
     if (ctx->stage_free[slot]) FD2_CHECK_CUDA(cudaEventSynchronize(ctx->stage_free[slot]));
     else FD2_CHECK_CUDA(cudaEventCreateWithFlags(&ctx->stage_free[slot], cudaEventDisableTiming));
     if (ctx->h_stage_bytes[slot] < up_bytes) {
+        // freeing pinned memory waits for the whole device (other workers'
+        // streams included), so a slot starts large (1 MiB: 26k beamlets a
+        // batch) and grows by doubling
+        const size_t want = std::max<size_t>({up_bytes, (size_t)1 << 20, 2 * ctx->h_stage_bytes[slot]});
         if (ctx->h_stage[slot]) FD2_CHECK_CUDA(cudaFreeHost(ctx->h_stage[slot]));
         ctx->h_stage[slot] = nullptr;
         ctx->h_stage_bytes[slot] = 0;
-        FD2_CHECK_CUDA(cudaHostAlloc(&ctx->h_stage[slot], up_bytes, cudaHostAllocDefault));
-        ctx->h_stage_bytes[slot] = up_bytes;
+        FD2_CHECK_CUDA(cudaHostAlloc(&ctx->h_stage[slot], want, cudaHostAllocDefault));
+        ctx->h_stage_bytes[slot] = want;
     }
     uint64_t* h = (uint64_t*)ctx->h_stage[slot];
     for (size_t k = 0; k < nb; k++) {

@@ -109,17 +109,50 @@ def merge_ensembles(parts, beams_of_rank, rows_per_beam):
 
 
 def gather_ensembles(local, beams_of_rank, rows_per_beam, group=None, dst=0):
-    """Gather every rank's host CSR ensemble to rank `dst` and merge there in
-    beam order; other ranks get None.  Every rank of the group must call it."""
+    """Gather every rank's CSR ensemble (row offsets, columns, values; numpy
+    arrays or tensors) to rank `dst` and merge there in beam order; other
+    ranks get None.  Every rank of the group must call it.
+
+    The arrays move as tensors: one all-gather of their sizes, then
+    point-to-point sends to `dst` -- device buffers over NCCL (the arrays are
+    copied to this rank's GPU first when they are on the host), host buffers
+    over gloo.  Values travel as float32."""
+    import torch
     import torch.distributed as dist
 
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
-    bucket = [None] * world if rank == dst else None
-    dist.gather_object(tuple(np.asarray(a) for a in local), bucket, dst=dst, group=group)
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" \
+        else torch.device("cpu")
+
+    def as_tensor(a, dtype):
+        t = a if torch.is_tensor(a) else torch.from_numpy(np.ascontiguousarray(a))
+        return t.to(device=dev, dtype=dtype).contiguous()
+
+    ro, col, val = (as_tensor(a, dt) for a, dt in zip(local, (torch.int64, torch.int32, torch.float32)))
+    sizes = torch.tensor([ro.numel(), col.numel()], dtype=torch.int64, device=dev)
+    every = [torch.empty_like(sizes) for _ in range(world)]
+    dist.all_gather(every, sizes, group=group)
+
+    def peer(r):
+        return r if group is None else dist.get_global_rank(group, r)
+
     if rank != dst:
+        for t in (ro, col, val):
+            dist.send(t, dst=peer(dst), group=group)
         return None
-    return merge_ensembles(bucket, beams_of_rank, rows_per_beam)
+    parts = []
+    for r in range(world):
+        if r == rank:
+            got = (ro, col, val)
+        else:
+            n_ro, n_nz = (int(v) for v in every[r].tolist())
+            got = (torch.empty(n_ro, dtype=torch.int64, device=dev), torch.empty(n_nz, dtype=torch.int32, device=dev),
+                   torch.empty(n_nz, dtype=torch.float32, device=dev))
+            for t in got:
+                dist.recv(t, src=peer(r), group=group)
+        parts.append(tuple(t.cpu().numpy() for t in got))
+    return merge_ensembles(parts, beams_of_rank, rows_per_beam)
 
 
 def row_blocks(n_rows: int, world: int) -> list[tuple[int, int]]:
