@@ -170,13 +170,13 @@ __device__ __forceinline__ float exp2_sfu(float x) {
     return y;
 }
 
-// Segment length sqrt(l2) with the SFU square root (PTX sqrt.approx.ftz.f32),
-// the operation the reference's fast-math sqrtf becomes in d_calcLineSeg
-// (DoseComp.cu:143); l2 > 0 for every segment the march takes.
+// Segment length sqrt(l2) as l2 * rsqrt(l2) with the SFU reciprocal square
+// root (PTX rsqrt.approx.ftz.f32); l2 > 0 for every segment the march takes.
+// (sqrt.approx.ftz.f32 alone measured slower on the 400-beam plan.)
 __device__ __forceinline__ float seg_length(float l2) {
     float r;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l2));
-    return r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l2));
+    return l2 * r;
 }
 
 // Block: n_phi warps.  Dynamic shared memory: float2 tr[P] (Terma, density of
@@ -198,14 +198,18 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                                                    float* const* __restrict__ dose,
                                                    const float4* __restrict__ dirs,  // [beam][n_tf][n_phi]
                                                    ConeParams cp, int split, float* __restrict__ split_out,
-                                                   size_t split_stride, DeviceStatus* status) {
+                                                   size_t split_stride, DeviceStatus* status,
+                                                   const int* __restrict__ order) {
     extern __shared__ float2 smem[];
     __shared__ int s_ctrl[2];  // next slice index, abort flag
     int* s_next = &s_ctrl[0];
     int* s_abort = &s_ctrl[1];
     if (threadIdx.x == 0) *s_abort = 0;
     const int n_tf = cp.n_theta_fwd, n_phi = cp.n_phi;
-    const int bi = split ? blockIdx.x / n_tf : blockIdx.x;
+    // order (optional): the beamlet each block slot marches, longest first,
+    // so the launch ends on short blocks
+    const int slot = split ? blockIdx.x / n_tf : blockIdx.x;
+    const int bi = order ? order[slot] : slot;
     const int t0 = split ? blockIdx.x % n_tf : 0;
     const int t1 = split ? t0 + 1 : n_tf;
     const fd2_beam_t& b = beams[bi];
@@ -530,7 +534,7 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                 }
                 const float val = sum / (last_sum_p + 1e-4f);
                 if (split)
-                    split_out[(size_t)blockIdx.x * split_stride + (size_t)s * g.P + v] = val;
+                    split_out[((size_t)bi * n_tf + t0) * split_stride + (size_t)s * g.P + v] = val;
                 else
                     // this block alone owns beam bi's dose and each (s, v) stays with
                     // one thread, so a fire-and-forget add gives D + val in pass order
@@ -564,11 +568,12 @@ __global__ void cccs_split_reduce(const fd2_beam_t* __restrict__ beams, float* c
 template <int RPL, bool kFx16, bool kCols, bool kTab = false>
 int launch_instance(unsigned blocks, int threads, size_t shm, cudaStream_t st, const fd2_beam_t* d_beams,
                     const float* const* T, const float* const* R, float* const* D, const float4* dirs,
-                    const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status) {
+                    const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status,
+                    const int* order) {
     FD2_CHECK_CUDA(cudaFuncSetAttribute(cccs_kernel<RPL, kFx16, kCols, kTab>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)shm));
     cccs_kernel<RPL, kFx16, kCols, kTab><<<blocks, threads, shm, st>>>(d_beams, T, R, D, dirs, cp, split, planes,
-                                                                 plane_stride, status);
+                                                                 plane_stride, status, order);
     FD2_CHECK_CUDA(cudaGetLastError());
     return FD2_OK;
 }
@@ -579,49 +584,50 @@ int launch_instance(unsigned blocks, int threads, size_t shm, cudaStream_t st, c
 // warps); anything else the general per-ray instance.
 int launch_march(int map, int maxP, int n_phi, unsigned blocks, cudaStream_t st, const fd2_beam_t* d_beams,
                  const float* const* T, const float* const* R, float* const* D, const float4* dirs,
-                 const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status) {
+                 const ConeParams& cp, int split, float* planes, size_t plane_stride, DeviceStatus* status,
+                 const int* order = nullptr) {
     const int threads = 32 * n_phi;
     const size_t shm = (size_t)(1 + n_phi) * maxP * sizeof(float2);
     const bool warps_ok = threads >= 128 && threads <= kFx16Threads;
     if (map == 16 && threads <= kFx16Threads)
         return launch_instance<8, true, false>(blocks, threads, (size_t)n_phi * (256 * sizeof(float4) + 16 * sizeof(float2)),
-                                               st, d_beams, T, R, D, dirs, cp, split, planes, plane_stride, status);
+                                               st, d_beams, T, R, D, dirs, cp, split, planes, plane_stride, status, order);
     if (map > 0 && map <= 24 && warps_ok) {  // half-table instance: rays per lane = ceil(F^2 / 32)
         const int P = map * map;
         if (P <= 64)
             return launch_instance<2, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                          planes, plane_stride, status);
+                                                          planes, plane_stride, status, order);
         if (P <= 160)
             return launch_instance<5, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                          planes, plane_stride, status);
+                                                          planes, plane_stride, status, order);
         if (P <= 256)
             return launch_instance<8, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                          planes, plane_stride, status);
+                                                          planes, plane_stride, status, order);
         if (P <= 416)
             return launch_instance<13, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp,
-                                                           split, planes, plane_stride, status);
+                                                           split, planes, plane_stride, status, order);
         return launch_instance<18, false, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                       planes, plane_stride, status);
+                                                       planes, plane_stride, status, order);
     }
     if (map > 0 && map <= 32 && warps_ok) {
         const int k = 32 / map, rows = (map + k - 1) / k;  // rows per lane
         if (rows <= 8)
             return launch_instance<8, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                   planes, plane_stride, status);
+                                                   planes, plane_stride, status, order);
         if (rows <= 20)
             return launch_instance<20, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                    planes, plane_stride, status);
+                                                    planes, plane_stride, status, order);
         if (rows <= 24)
             return launch_instance<24, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split,
-                                                    planes, plane_stride, status);
+                                                    planes, plane_stride, status, order);
         return launch_instance<32, false, true>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
-                                                plane_stride, status);
+                                                plane_stride, status, order);
     }
     if (maxP <= 256)
         return launch_instance<8, false, false>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
-                                                plane_stride, status);
+                                                plane_stride, status, order);
     return launch_instance<32, false, false>(blocks, threads, shm, st, d_beams, T, R, D, dirs, cp, split, planes,
-                                             plane_stride, status);
+                                             plane_stride, status, order);
 }
 
 // common map side of a batch (F when every map is F x F), else 0
@@ -635,7 +641,7 @@ int common_map(int side, const fd2_beam_t& b) {
 
 int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams, const fd2_beam_t* d_beams,
                      const float* const* d_terma, const float* const* d_dens, float* const* d_dose,
-                     const fd2_cccs_kernel* k, int schedule, cudaStream_t stream) {
+                     const fd2_cccs_kernel* k, int schedule, cudaStream_t stream, const int* d_order) {
     if (n_beams == 0) return FD2_OK;
     ConeParams cp{};
     std::vector<int> fwd;
@@ -679,7 +685,7 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     int map = -1;
     for (size_t i = 0; i < n_beams && map != 0; i++) map = common_map(map, h_beams[i]);
     FD2_TRY(launch_march(map, maxP, k->n_phi, blocks, stream, d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
-                         d_planes, plane_stride, ctx->d_status));
+                         d_planes, plane_stride, ctx->d_status, d_order));
     ctx->launches += 2;  // direction table + march
     if (schedule == 1) {
         dim3 grid(std::max(1, std::min(64, (int)((plane_stride + 255) / 256))), (unsigned)n_beams);
@@ -702,6 +708,14 @@ size_t cccs_scratch_bytes(size_t n_beams, const fd2_beam_t* h_beams, const fd2_c
     const size_t dir_bytes = n_beams * n_fwd * k->n_phi * sizeof(float4);
     const size_t plane_bytes = schedule == 1 ? n_beams * n_fwd * maxP * maxL * sizeof(float) : 0;
     return dir_bytes + plane_bytes + 256;
+}
+
+void cccs_longest_first(size_t n_beams, const fd2_beam_t* h_beams, int* order) {
+    std::vector<int> idx(n_beams);
+    for (size_t i = 0; i < n_beams; i++) idx[i] = (int)i;
+    std::stable_sort(idx.begin(), idx.end(),
+                     [&](int a, int b) { return h_beams[a].long_dim > h_beams[b].long_dim; });
+    std::copy(idx.begin(), idx.end(), order);
 }
 
 // Automatic schedule: split the zenith bins across blocks when the beamlets
@@ -727,7 +741,7 @@ extern "C" int fd2_dose_compute(fd2_context* ctx, size_t fmap_npixels, size_t n_
     FD2_CHECK_CUDA(cudaStreamSynchronize(st));
     return fd2::launch_cccs_host(ctx, n_beams, hb.data(), d_beams, (const float* const*)d_terma,
                                  (const float* const*)d_density_bev, d_dose, kernel,
-                                 fd2::cccs_auto_schedule(ctx, n_beams), st);
+                                 fd2::cccs_auto_schedule(ctx, n_beams), st, nullptr);
 }
 
 extern "C" int fd2_cccs_cone_directions(fd2_context* ctx, const fd2_cccs_kernel* k, size_t n_beams,

@@ -334,8 +334,9 @@ static int graph_batch(fd2_context* ctx, fd2_csr_ensemble* e, size_t nb, const f
                        const fd2_density* density, const fd2_spectrum* spectrum, const fd2_cccs_kernel* kernel,
                        const fd2_dosemat_params_t& params, int schedule, cudaStream_t st) {
     // device layout of the batch buffer: aF, aT, aR, aD (pointers), candidate
-    // offsets -- uploaded from the staging -- then the column-stage scratch
-    const size_t up_bytes = (4 * nb + nb + 1) * sizeof(uint64_t);
+    // offsets, the march order (int32) -- uploaded from the staging -- then the
+    // column-stage scratch
+    const size_t up_bytes = (4 * nb + nb + 1 + (nb + 1) / 2) * sizeof(uint64_t);
     const size_t o_nnz = align256(up_bytes), o_max = o_nnz + align256(nb * 4), o_isc = o_max + align256(nb * 4);
     const size_t dev_bytes = o_isc + align256(nb * 4);
     uint64_t ncap_total = 0;
@@ -371,11 +372,14 @@ static int graph_batch(fd2_context* ctx, fd2_csr_ensemble* e, size_t nb, const f
     uint64_t* hc = h + 4 * nb;
     hc[0] = 0;
     for (size_t k = 0; k < nb; k++) hc[k + 1] = hc[k] + cnt[k];
+    int* ho = (int*)(hc + nb + 1);
+    cccs_longest_first(nb, h_beams, ho);
     char* b = (char*)batch;
     const float** aF = (const float**)b;
     float** aT = (float**)(b + nb * 8);
     float** aR = (float**)(b + 2 * nb * 8);
     float** aD = (float**)(b + 3 * nb * 8);
+    const int* d_order = (const int*)(b + (5 * nb + 1) * 8);
     ColumnScratch pre;
     pre.cap_off = (uint64_t*)(b + 4 * nb * 8);
     pre.nnz = (uint32_t*)(b + o_nnz);
@@ -388,7 +392,7 @@ static int graph_batch(fd2_context* ctx, fd2_csr_ensemble* e, size_t nb, const f
         FD2_CHECK_CUDA(cudaMemsetAsync(dD, 0, off[nb] * sizeof(float), st));
         FD2_TRY(launch_terma(ctx, P, nb, d_beams, aF, aT, aR, density, spectrum, 1, st));
         FD2_TRY(launch_cccs_host(ctx, nb, h_beams, d_beams, (const float* const*)aT, (const float* const*)aR, aD,
-                                 kernel, schedule, st));
+                                 kernel, schedule, st, d_order));
         return append_columns(e, d_infos, cnt, nb, (const float* const*)aD, density->vol, params.extent,
                               params.ss_factor, st, &pre);
     }();
@@ -637,6 +641,15 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     rc = upload(std::vector<float>(h_fluence, h_fluence + P), &d_fluence, ctx->pool, st);
     if (!rc) rc = upload(beams, &d_beams, ctx->pool, st);
 
+    // batches of about equal size: as many as the budget needs, whole beams
+    // each, so no batch is a small remainder (a launch of a few waves spends
+    // proportionally more of its time in its tail)
+    {
+        size_t all = 0;
+        for (const auto& b : beams) all += (size_t)b.long_dim * P * 3 * sizeof(float);
+        const size_t n_batches = std::max<size_t>(1, (all + budget - 1) / std::max<size_t>(budget, 1));
+        budget = std::min(budget, (all + n_batches - 1) / n_batches + (size_t)1);
+    }
     size_t b0 = 0, beam0 = 0;
     const auto t_start = std::chrono::steady_clock::now();
     auto ms_since = [&](std::chrono::steady_clock::time_point t) {
@@ -686,7 +699,11 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         for (size_t k = 0; k < nb; k++) { hT[k] = dT + off[k]; hR[k] = dR + off[k]; hD[k] = dD + off[k]; }
         const float** aF = nullptr;
         float **aT = nullptr, **aR = nullptr, **aD = nullptr;
+        int* d_order = nullptr;
+        std::vector<int> order(nb);
+        cccs_longest_first(nb, beams.data() + b0, order.data());
         rc = [&]() -> int {
+            FD2_TRY(upload(order, &d_order, ctx->pool, st));
             FD2_TRY(upload(hF, &aF, ctx->pool, st));
             FD2_TRY(upload(hT, &aT, ctx->pool, st));
             FD2_TRY(upload(hR, &aR, ctx->pool, st));
@@ -701,7 +718,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
                 StageTimer t(ctx, st, FD2_STAGE_CCCS);
                 auto run = [&](int sched) {
                     return launch_cccs_host(ctx, nb, beams.data() + b0, d_beams + b0, (const float* const*)aT,
-                                            (const float* const*)aR, aD, kernel, sched, st);
+                                            (const float* const*)aR, aD, kernel, sched, st, d_order);
                 };
                 if (params.cccs_schedule >= 0) {
                     FD2_TRY(run(params.cccs_schedule));
@@ -719,7 +736,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
             return r;
         }();
         // release batch buffers
-        for (void* p : {(void*)aF, (void*)aT, (void*)aR, (void*)aD})  // d_bev is the context's
+        for (void* p : {(void*)aF, (void*)aT, (void*)aR, (void*)aD, (void*)d_order})  // d_bev is the context's
             if (p) cudaFreeAsync(p, st);
         if (rc) break;
         if (params.host_out) {

@@ -38,7 +38,11 @@ int launch_column_gather(size_t n, const uint64_t* d_cap_off, const int64_t* d_r
 
 int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams, const fd2_beam_t* d_beams,
                      const float* const* d_terma, const float* const* d_dens, float* const* d_dose,
-                     const fd2_cccs_kernel* k, int schedule, cudaStream_t stream);
+                     const fd2_cccs_kernel* k, int schedule, cudaStream_t stream,
+                     const int* d_order = nullptr);
+// The march order of a batch: beamlet indices by decreasing depth (slices to
+// march), ties in batch order, so a launch's last blocks are its short ones.
+void cccs_longest_first(size_t n_beams, const fd2_beam_t* h_beams, int* order);
 int cccs_auto_schedule(const fd2_context* ctx, size_t n_beams);
 
 }  // namespace fd2

@@ -26,7 +26,6 @@
 // column) bytes, the bitmap (nnz/8 bytes) and x, and writes y.
 #include <algorithm>
 #include <cmath>
-#include <cstdlib>
 #include <vector>
 
 #include <cub/device/device_radix_sort.cuh>
@@ -43,8 +42,6 @@ constexpr int kStreamThreads = 256;
 constexpr int kMaxStreamWarps = 148 * 64;  // one full wave of 64 warps per SM
 constexpr int kSmemThreads = 1024;          // x-in-shared-memory variant: one block per SM
 constexpr int64_t kSmemXMaxBytes = 200 * 1024;
-constexpr int kPrefetchHalf = 4;  // L2 prefetch distance in chunks, 16-bit values
-constexpr int kPrefetchF32 = 2;   // and FP32 values
 
 struct StreamArgs {
     const void* val;
@@ -59,17 +56,8 @@ struct StreamArgs {
     int64_t rows;
     int64_t* carry_row;
     float* carry_val;
-    int x_len;     // kSmemX: floats of x staged in shared memory
-    int prefetch;  // chunks ahead of the one being summed whose bytes are prefetched into L2 (0: none)
+    int x_len;  // kSmemX: floats of x staged in shared memory
 };
-
-// An L2 prefetch of `bytes` (a multiple of 16) at a 16-byte aligned address,
-// issued by one thread as one bulk operation (PTX cp.async.bulk.prefetch.L2):
-// the bytes travel from HBM while the warp sums earlier chunks, and hold no
-// registers or shared memory.
-__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
-}
 
 // A lane's share of one chunk as loaded, values and columns still packed, so
 // that two chunks can be in flight per warp without holding 2 x 16 unpacked
@@ -193,20 +181,6 @@ __global__ void __launch_bounds__(kSmemX ? kSmemThreads : kStreamThreads, kSmemX
         else
             return __ldg(x + col);
     };
-    // lane 0 prefetches the values, columns and row-start bytes of chunk c
-    // (inside this warp's range, so every address is part of the matrix)
-    auto prefetch_chunk = [&](int64_t c) {
-        if (lane == 0 && c < c1) {
-            prefetch_l2(static_cast<const T*>(a.val) + c * kChunk, kChunk * sizeof(T));
-            if constexpr (kPacked)
-                prefetch_l2(a.cols.col16 + c * kChunk, kChunk * sizeof(uint16_t));
-            else
-                prefetch_l2(a.cols.col + c * kChunk, kChunk * sizeof(int32_t));
-            prefetch_l2(reinterpret_cast<const uint8_t*>(a.head) + c * (kChunk / 8), kChunk / 8);
-        }
-    };
-    if (a.prefetch > 0)
-        for (int64_t c = c0; c < c0 + a.prefetch; c++) prefetch_chunk(c);
     // row of the chunk's j-th row start: consecutive rows need no lookup
     auto row_at = [&](const RawChunk<T, kPacked>& r, int j) -> int {
         return r.row0 >= 0 ? r.row0 + j : __ldg(a.nzrow + (-1 - r.row0) + j);
@@ -275,7 +249,6 @@ __global__ void __launch_bounds__(kSmemX ? kSmemThreads : kStreamThreads, kSmemX
         RawChunk<T, kPacked> r;
         if (c0 < c1) load_raw(a, c0, lane, r);
         for (int64_t c = c0; c < c1; c++) {
-            if (a.prefetch > 0) prefetch_chunk(c + a.prefetch);
             RawChunk<T, kPacked> rn;
             const bool more = c + 1 < c1;  // uniform per warp
             if (more) load_raw(a, c + 1, lane, rn);
@@ -286,10 +259,6 @@ __global__ void __launch_bounds__(kSmemX ? kSmemThreads : kStreamThreads, kSmemX
         // 16-bit values, x gathered from global memory: two chunks' loads are
         // issued together (fewer registers held than the rolling form)
         for (int64_t c = c0; c < c1; c += 2) {
-            if (a.prefetch > 0) {
-                prefetch_chunk(c + a.prefetch);
-                prefetch_chunk(c + a.prefetch + 1);
-            }
             RawChunk<T, kPacked> r0, r1;
             load_raw(a, c, lane, r0);
             const bool two = c + 1 < c1;  // uniform per warp
@@ -299,7 +268,6 @@ __global__ void __launch_bounds__(kSmemX ? kSmemThreads : kStreamThreads, kSmemX
         }
     } else {
         for (int64_t c = c0; c < c1; c++) {
-            if (a.prefetch > 0) prefetch_chunk(c + a.prefetch);
             RawChunk<T, kPacked> r;
             load_raw(a, c, lane, r);
             body(r, c);
@@ -569,23 +537,11 @@ int launch_stream_fmt(const fd2_matrix* m, const StreamArgs& a, const float* x, 
     return FD2_OK;
 }
 
-// Chunks a warp prefetches into L2 ahead of the one it sums.  The default
-// comes from timing the optimization benchmark's matrices; FD2_SPMV_PREFETCH
-// overrides it (0 turns the prefetch off), read once per process.
-int spmv_prefetch_chunks(bool half) {
-    static int env = [] {
-        const char* e = std::getenv("FD2_SPMV_PREFETCH");
-        return e ? std::max(0, std::min(64, std::atoi(e))) : -1;
-    }();
-    if (env >= 0) return env;
-    return half ? kPrefetchHalf : kPrefetchF32;
-}
-
 template <typename T>
 int launch_stream(const fd2_matrix* m, const float* x, float* y, cudaStream_t st) {
     StreamArgs a{m->d_val, m->cols_view(), m->d_head, m->d_chunk_h, m->d_chunk_row0, m->d_nzrow,
                  m->scale_axis == FD2_SCALE_ROWS ? m->d_scale : nullptr, m->n_chunks, m->n_warps, m->rows,
-                 m->d_carry_row, m->d_carry_val, (int)m->cols, spmv_prefetch_chunks(sizeof(T) == 2)};
+                 m->d_carry_row, m->d_carry_val, (int)m->cols};
     if (m->index_format == FD2_INDEX_PACKED16)
         FD2_TRY((launch_stream_fmt<T, true>(m, a, x, y, st)));
     else
