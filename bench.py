@@ -651,7 +651,7 @@ def _lat_stats(lat_s):
 
 
 def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_per_rate=20.0, seed=11, workers=2,
-               plain_requests=30, graph_off_rate=10.0):
+               plain_requests=30, graph_rate=10.0):
     """p50/p99 plan latency (arrival -> dose-loading matrix on the device) and
     beamlets/s of the service under Poisson arrivals at each rate, over
     min(n_requests, max(30, rate * seconds_per_rate)) requests (seconds_per_rate
@@ -660,8 +660,8 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
     first plain_requests requests.  At higher rates the plain single server is
     overloaded (its utilisation, rate x mean service time, is reported); its
     latencies there are a FIFO replay of the service times measured live.
-    The service launches each construction batch as one CUDA graph; at
-    graph_off_rate the same arrivals also run with kernel-by-kernel launches."""
+    The service launches kernel by kernel; at graph_rate the same arrivals
+    also run with each construction batch launched as one CUDA graph."""
     import threading
 
     import torch
@@ -757,7 +757,7 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
 
     for lam in rates:
         n = len(reqs) if seconds_per_rate <= 0 else min(len(reqs), max(30, int(lam * seconds_per_rate)))
-        arr, svc_stats = run_rate(lam, n, graph=True)
+        arr, svc_stats = run_rate(lam, n, graph=False)
         # the plain single server at this rate: FIFO replay of the live service times
         end, rl = 0.0, []
         for a, sv in zip(arr[:n_plain], service_s):
@@ -773,11 +773,11 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
         if lam == 1.0:
             out[key]["plain_single_beam"].update({k: plain_live[k] for k in ("p50_ms", "p99_ms", "max_ms")},
                                                  basis="live")
-    if graph_off_rate:
-        n = min(len(reqs), max(30, int(graph_off_rate * seconds_per_rate))) if seconds_per_rate > 0 else len(reqs)
-        _, off = run_rate(graph_off_rate, n, graph=False)  # the same arrivals, kernel-by-kernel launches
-        off.pop("timeline")
-        out[f"rate_{graph_off_rate:g}_per_s"]["service_without_graphs"] = off
+    if graph_rate and f"rate_{graph_rate:g}_per_s" in out:
+        n = min(len(reqs), max(30, int(graph_rate * seconds_per_rate))) if seconds_per_rate > 0 else len(reqs)
+        _, on = run_rate(graph_rate, n, graph=True)  # the same arrivals, one graph per construction batch
+        on.pop("timeline")
+        out[f"rate_{graph_rate:g}_per_s"]["service_with_graphs"] = on
     svc.close()
     return out
 

@@ -172,7 +172,6 @@ __device__ __forceinline__ float exp2_sfu(float x) {
 
 // Segment length sqrt(l2) as l2 * rsqrt(l2) with the SFU reciprocal square
 // root (PTX rsqrt.approx.ftz.f32); l2 > 0 for every segment the march takes.
-// (sqrt.approx.ftz.f32 alone measured slower on the 400-beam plan.)
 __device__ __forceinline__ float seg_length(float l2) {
     float r;
     asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(l2));
@@ -206,10 +205,9 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
     int* s_abort = &s_ctrl[1];
     if (threadIdx.x == 0) *s_abort = 0;
     const int n_tf = cp.n_theta_fwd, n_phi = cp.n_phi;
-    // order (optional): the beamlet each block slot marches, longest first,
-    // so the launch ends on short blocks
-    const int slot = split ? blockIdx.x / n_tf : blockIdx.x;
-    const int bi = order ? order[slot] : slot;
+    // order (optional, one block per beamlet only): the beamlet each block
+    // marches, longest first, so the launch ends on short blocks
+    const int bi = split ? blockIdx.x / n_tf : (order ? order[blockIdx.x] : blockIdx.x);
     const int t0 = split ? blockIdx.x % n_tf : 0;
     const int t1 = split ? t0 + 1 : n_tf;
     const fd2_beam_t& b = beams[bi];
@@ -242,7 +240,6 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
     float2* tr = smem;
     float2* dp = smem + g.P;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool last_phi = warp == n_phi - 1;  // uniform per warp
     float2* mydp = dp + (size_t)warp * g.P;
     // kFx16: every azimuth warp keeps its own copy of the slice beside its sums,
     // wb[warp][v] = {Terma, density, dose, path sum}, so a ray step reads all
@@ -371,12 +368,7 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                         const float p = len * e.y;
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
-                        // only the last azimuth's path sums are read (quirk Q2): the
-                        // other warps keep the dose alone
-                        if (last_phi)
-                            *reinterpret_cast<float2*>(&v->z) = make_float2(e.z + dep, e.w + p);
-                        else
-                            v->z = e.z + dep;
+                        *reinterpret_cast<float2*>(&v->z) = make_float2(e.z + dep, e.w + p);
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - e.x, e.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - e.x, e.x);
                     };
@@ -410,14 +402,10 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                         const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                         if (on) {
-                            if (last_phi) {
-                                float2 acc = mydp[mi];
-                                acc.x += dep;
-                                acc.y += p;
-                                mydp[mi] = acc;
-                            } else {
-                                mydp[mi].x += dep;
-                            }
+                            float2 acc = mydp[mi];
+                            acc.x += dep;
+                            acc.y += p;
+                            mydp[mi] = acc;
                         }
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
@@ -459,14 +447,10 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                         const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                         if (on) {
                             float2* acc_p = reinterpret_cast<float2*>(reinterpret_cast<char*>(mydp) + mb);
-                            if (last_phi) {
-                                float2 acc = *acc_p;
-                                acc.x += dep;
-                                acc.y += p;
-                                *acc_p = acc;
-                            } else {
-                                acc_p->x += dep;
-                            }
+                            float2 acc = *acc_p;
+                            acc.x += dep;
+                            acc.y += p;
+                            *acc_p = acc;
                         }
                         XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                         XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
@@ -490,14 +474,10 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                     const float ea = exp2_sfu(ka * p), eb = exp2_sfu(kb * p);
                     const float dep = (Aa * XA[j] + Bb * XB[j]) * p;
                     if (act[j]) {
-                        if (last_phi) {
-                            float2 acc = mydp[mi];
-                            acc.x += dep;
-                            acc.y += p;
-                            mydp[mi] = acc;
-                        } else {
-                            mydp[mi].x += dep;
-                        }
+                        float2 acc = mydp[mi];
+                        acc.x += dep;
+                        acc.y += p;
+                        mydp[mi] = acc;
                     }
                     XA[j] = wrap ? 0.0f : __fmaf_rn(ea, XA[j] - trv.x, trv.x);
                     XB[j] = wrap ? 0.0f : __fmaf_rn(eb, XB[j] - trv.x, trv.x);
@@ -534,7 +514,7 @@ __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
                 }
                 const float val = sum / (last_sum_p + 1e-4f);
                 if (split)
-                    split_out[((size_t)bi * n_tf + t0) * split_stride + (size_t)s * g.P + v] = val;
+                    split_out[(size_t)blockIdx.x * split_stride + (size_t)s * g.P + v] = val;
                 else
                     // this block alone owns beam bi's dose and each (s, v) stays with
                     // one thread, so a fire-and-forget add gives D + val in pass order
@@ -685,7 +665,7 @@ int launch_cccs_host(fd2_context* ctx, size_t n_beams, const fd2_beam_t* h_beams
     int map = -1;
     for (size_t i = 0; i < n_beams && map != 0; i++) map = common_map(map, h_beams[i]);
     FD2_TRY(launch_march(map, maxP, k->n_phi, blocks, stream, d_beams, d_terma, d_dens, d_dose, d_dirs, cp, schedule,
-                         d_planes, plane_stride, ctx->d_status, d_order));
+                         d_planes, plane_stride, ctx->d_status, schedule == 1 ? nullptr : d_order));
     ctx->launches += 2;  // direction table + march
     if (schedule == 1) {
         dim3 grid(std::max(1, std::min(64, (int)((plane_stride + 255) / 256))), (unsigned)n_beams);
