@@ -35,7 +35,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "CCCS beamlets/s (dose-loading matrix, batched 4pi)"
-CCCS_DRAM_BYTES_PER_BEAMLET = 3.7754e9 / 610
+# From one ncu capture of the CCCS march on the 40-beam plan (6056 beamlets,
+# 8.2 waves; profiles/cccs_kernel_4pi_torso_40beams.md):
+# dram__bytes_read.sum + dram__bytes_write.sum, and smsp__inst_executed.sum
+CCCS_DRAM_BYTES_PER_BEAMLET = (28.925890e9 + 9.509276e9) / 6056
+CCCS_WARP_INST_PER_BEAMLET = 141.212517619e9 / 6056
 UNIT = "beamlets/s"
 
 
@@ -167,8 +171,11 @@ def cpu_baseline(cfg, beamlets, fluence, budget_s, threads, start=0, order=None)
 
 
 def workload_name(n_beams, n_beamlets):
-    """The bench workload, named the same by both arms."""
-    return (f"4pi torso 200x200x160 @2.5mm, {n_beams} beams, {n_beamlets} beamlets (16x16, 0.5 cm), "
+    """The bench workload, named the same by both arms (the beamlet count is
+    its own config key: the reference arm flags beamlets with the host
+    restatement of the texture test, which may differ in a beamlet or two)."""
+    del n_beamlets
+    return (f"4pi torso 200x200x160 @2.5mm, {n_beams} beams, 16x16 beamlets of 0.5 cm flagged by the PTV, "
             f"8x6 cones, 12-bin spectrum")
 
 
@@ -659,9 +666,12 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
     time, one beam per construction call -- run live at 1 request/s over the
     first plain_requests requests.  At higher rates the plain single server is
     overloaded (its utilisation, rate x mean service time, is reported); its
-    latencies there are a FIFO replay of the service times measured live.
+    latencies there are a FIFO replay of its service times of the same
+    requests, measured live at 1/s for the first plain_requests and back to
+    back for the rest.
     The service launches kernel by kernel; at graph_rate the same arrivals
-    also run with each construction batch launched as one CUDA graph."""
+    also run with each construction batch launched as one CUDA graph.  Before
+    the sweep, the first 48 requests run once untimed in both forms."""
     import threading
 
     import torch
@@ -701,10 +711,16 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
         end = time.perf_counter()
         service_s.append(end - s0)
         lat.append(end - t0 - a)
-    mean_s = float(np.mean(service_s))
     plain_live = dict(_lat_stats(lat), rate_per_s=1.0, beamlets_per_s=sum(n_bl[:n_plain]) / (time.perf_counter() - t0),
-                      mean_service_ms=1e3 * mean_s)
+                      mean_service_ms=1e3 * float(np.mean(service_s)))
     out["plain_live_1_per_s"] = plain_live
+    # the plain form's service time of every other request the sweep runs,
+    # back to back, so that its replay at each rate covers the same requests
+    n_max = len(reqs) if seconds_per_rate <= 0 else min(len(reqs), max(30, int(max(rates) * seconds_per_rate)))
+    for r in reqs[n_plain:n_max]:
+        s0 = time.perf_counter()
+        plain_run(r)
+        service_s.append(time.perf_counter() - s0)
 
     svc = service.Service(device=torch.cuda.current_device(), workers=workers)
     big = int(np.argmax(n_bl))
@@ -718,6 +734,14 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
             warmed.add(int(s["worker"]))
         if len(warmed) == workers:
             break
+    # one untimed pass over the request pool, kernel by kernel and with graphs,
+    # so that the first rate of the sweep does not pay the workers' first-touch
+    # allocations and graph instantiations that later rates no longer see
+    for graph in (False, True):
+        tickets = [svc.submit(r["phantom"], r["beams"], r["fluence"], spec, kern, graph=graph)
+                   for r in reqs[:min(len(reqs), 48)]]
+        for t in tickets:
+            svc.wait(t)[0].close()
     arrivals = {}
 
     def run_rate(lam, n, graph):
@@ -758,17 +782,19 @@ def served_leg(ctx, rates=(1.0, 5.0, 10.0, 20.0, 50.0), n_requests=200, seconds_
     for lam in rates:
         n = len(reqs) if seconds_per_rate <= 0 else min(len(reqs), max(30, int(lam * seconds_per_rate)))
         arr, svc_stats = run_rate(lam, n, graph=False)
-        # the plain single server at this rate: FIFO replay of the live service times
+        # the plain single server at this rate: FIFO replay of its measured
+        # service times of the same n requests
         end, rl = 0.0, []
-        for a, sv in zip(arr[:n_plain], service_s):
+        for a, sv in zip(arr[:n], service_s[:n]):
             end = max(end, a) + sv
             rl.append(end - a)
         key = f"rate_{lam:g}_per_s"
         out[key] = {
             "service": svc_stats,
-            "plain_single_beam": dict(_lat_stats(rl), utilisation=lam * mean_s,
+            "plain_single_beam": dict(_lat_stats(rl), utilisation=lam * float(np.mean(service_s[:n])), requests=n,
                                       basis="live" if lam == 1.0 else
-                                      f"FIFO replay of the {n_plain} live service times at this rate"),
+                                      f"FIFO replay at this rate of the plain form's service times of the same "
+                                      f"{n} requests (the first {n_plain} timed live at 1/s, the rest back to back)"),
         }
         if lam == 1.0:
             out[key]["plain_single_beam"].update({k: plain_live[k] for k in ("p50_ms", "p99_ms", "max_ms")},
@@ -983,7 +1009,7 @@ def run_fd2(args, rank, world):
     L = np.concatenate([b["long_dim"] for b in beamlets]).astype(np.float64)
     cccs_bytes = float(np.sum(4.0 * P * L * 3))  # Terma + density read, dose written, per beamlet
     # DRAM bytes the CCCS kernel moves per beamlet: dram__bytes_read.sum + dram__bytes_write.sum of one
-    # ncu capture of the march on the 4-beam plan (610 beamlets, 3.78 GB),
+    # ncu capture of the march on the 40-beam plan (6056 beamlets, 38.4 GB),
     # scaled by the beamlets of this step (each zenith pass re-reads its slices: traffic grows with beamlets)
     cccs_traffic = CCCS_DRAM_BYTES_PER_BEAMLET * n_bl
     cccs_ms = stages["cccs"]
@@ -1002,6 +1028,13 @@ def run_fd2(args, rank, world):
     sm_mhz = clk_now.get("sm_mhz") or 1965.0
     sfu_peak = 16.0 * (torch.cuda.get_device_properties(dev).multi_processor_count) * sm_mhz * 1e6
     sfu_achieved = sfu_ops / (cccs_ms * 1e-3) if cccs_ms > 0 else None
+    # The march's binding roof is instruction issue: warp instructions per
+    # beamlet from the ncu capture, over the CUDA-event CCCS time, against 4
+    # warp instructions per clock per SM (one per sub-partition) at the sampled
+    # SM clock.
+    issue_inst = CCCS_WARP_INST_PER_BEAMLET * n_bl
+    issue_peak = 4.0 * torch.cuda.get_device_properties(dev).multi_processor_count * sm_mhz * 1e6
+    issue_achieved = issue_inst / (cccs_ms * 1e-3) if cccs_ms > 0 else None
     # The whole pipeline against HBM under the compulsory-traffic convention:
     # per beamlet Terma and density written and read, dose written and read
     # (4 P L 6), the density footprint read once (taken as its nonzero count),
@@ -1028,6 +1061,12 @@ def run_fd2(args, rank, world):
                          "frac": sfu_achieved / sfu_peak if sfu_achieved else None,
                          "basis": "3 MUFU per ray step; ray steps L (1 + (|dx|+|dy|)/dz) per cone pass from the "
                                   "device's cone directions; peak 16/clk/SM at the sampled SM clock"},
+        "issue_roofline": {"bound": "issue", "kernel": "cccs_kernel", "warp_instructions_per_step": issue_inst,
+                           "achieved": issue_achieved, "peak": issue_peak, "unit": "warp instructions/s",
+                           "frac": issue_achieved / issue_peak if issue_achieved else None,
+                           "basis": "warp instructions per beamlet from one ncu capture of the 40-beam plan "
+                                    "(smsp__inst_executed.sum / beamlets), scaled by this step's beamlets; "
+                                    "peak 4 per clock per SM at the sampled SM clock"},
         "pipeline_roofline": {"bound": "hbm", "bytes_per_step": pipe_bytes, "ms_per_step": pipe_ms,
                               "achieved": pipe_bytes / (pipe_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                               "frac": pipe_bytes / (pipe_ms * 1e-3) / 1e9 / peak,

@@ -12,11 +12,14 @@ oracle/build_ref.sh) on a GPU:
                       six oblique beams -- Terma and dose BEV of the first,
                       the interpolated dose column of both
   bev2pvcs_ss_ref.npz fastdose::BEV2PVCS_SuperSampling of config-1 beamlet 44
+  dose_c4_ref.npz     the multi-isocentre case: two beamlets each from two
+                      isocentres with 24x24 sub-beam maps (Terma, density and
+                      dose BEV, columns)
   reference_timings.json  kernel times, and IMRT::DoseMatConstruction's steps
                       over the whole 4pi plan (part "c2full")
 
 Usage (on a GPU machine): python tests/golden/make_golden_dose.py OUTDIR [part ...]
-with parts from c1 small flags c2timing c2 ss c2full (default: all).  The
+with parts from c1 small flags c2timing c2 ss c2full c4 (default: all).  The
 fixtures are then copied next to this script; reference_timings.json is
 updated in place, keeping the keys of parts not rerun.
 """
@@ -224,7 +227,55 @@ def c2full(outdir):
                 c2full_beamlets_per_s=r["beamlets"] / (float(t[4]) * 1e-3))
 
 
-PARTS = ("c1", "small", "flags", "c2timing", "c2", "ss", "c2full")
+C4_MAPS = (24, 16, 24, 16)
+
+
+def c4(outdir):
+    """Two beamlets each from isocentres 0 and 2 of the small multi-isocentre
+    head-and-neck case, with 24x24 sub-beam maps, through the reference's
+    Terma, CCCS and batched interpolation with the 8x8 kernel.
+
+    The reference's CCCS block has one thread per map pixel rounded up to a
+    warp, and the threads past the map return (DoseComp.cu:236) before the
+    block-wide barriers and the block-wide async slice copy (DoseComp.cu:295,
+    305-309, 382).  Maps whose pixel count is not a multiple of 32 (12x12,
+    20x20) are therefore outside its defined behaviour and are not run here.
+    24x24 (576 pixels) is, and at 8 azimuths its dynamic shared memory
+    (20 x 576 x 4 + 192 bytes) stays under the 48 KB the launch gets without
+    an opt-in (DoseComp.cu:203-205)."""
+    from fastdose_b200 import api
+
+    cfg = phantoms.config4(n_per_iso=3, dim=(64, 64, 50), sub_fluence_dims=C4_MAPS)
+    ph = cfg["phantom"]
+    kern = ref_kernel()
+    keep = {}
+    for k in (0, 2):
+        iso = cfg["isos"][k]
+        fd = int(iso["fluence_dims"][1])
+        bb = make_bundle(iso["isocenter"], iso["angles"][1], sad=cfg["sad"], fluence_dim=fd,
+                         beamlet_size=cfg["beamlet_size"], sub_fluence_dim=iso["sub_fluence_dim"],
+                         sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+        flags = np.zeros(fd * fd, np.uint8)
+        flags[(fd // 2) * fd + fd // 2] = flags[(fd // 2 - 1) * fd + fd // 2 - 1] = 1  # two central beamlets
+        beams = api.bundle_beamlets(bb, flags, ph.volume)
+        log("c4: isocentre", k, "map", iso["sub_fluence_dim"], "long_dim", beams["long_dim"])
+        r = ref.dose_batch(beams, api.beamlet_fluence(bb), ph.density, ph.volume, cfg["spectrum"], kern,
+                           extent=cfg["extent"], dense=True)
+        assert r["status"] == 0, r["status"]
+        keep[f"beams_{k}"] = beams
+        keep[f"fluence_{k}"] = api.beamlet_fluence(bb)
+        for j in range(2):
+            L = int(beams[j]["long_dim"])
+            keep[f"terma_{k}_{j}"] = r["terma"][j, :L]
+            keep[f"dens_{k}_{j}"] = r["dens"][j, :L]
+            keep[f"dose_{k}_{j}"] = r["dose"][j, :L]
+            nz = np.nonzero(r["dense"][j])[0]
+            keep[f"col_{k}_{j}"] = nz.astype(np.int32)
+            keep[f"val_{k}_{j}"] = r["dense"][j, nz]
+    np.savez_compressed(os.path.join(outdir, "dose_c4_ref.npz"), kernel_phi=kern.phi, **keep)
+
+
+PARTS = ("c1", "small", "flags", "c2timing", "c2", "ss", "c2full", "c4")
 
 
 def main():
@@ -239,7 +290,7 @@ def main():
     if os.path.exists(path):
         with open(path) as f:
             meta = json.load(f)
-    fns = dict(c1=c1, small=small, flags=flags, c2timing=c2_timing, c2=c2, ss=ss, c2full=c2full)
+    fns = dict(c1=c1, small=small, flags=flags, c2timing=c2_timing, c2=c2, ss=ss, c2full=c2full, c4=c4)
     for p in parts:
         got = fns[p](outdir)
         if got:
