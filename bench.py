@@ -1093,16 +1093,19 @@ def run_fd2(args, rank, world):
                 "batch_beamlets": int(e2e_batch), "read_back": "pinned, overlapped with the next batch"},
         "clocks": clk_now,
     }
-    if not args.no_extras:
+    if world > 1 and not args.no_extras:
+        # the single-GPU legs (one beam per call, reference CUDA, optimizer,
+        # C4, served) belong to the 1-GPU line; a multi-GPU run times the
+        # sharded construction only
+        line["extras"] = "single-GPU legs are reported by the 1-GPU run"
+    if world == 1 and not args.no_extras:
         sb = single_beam_leg(ctx, beamlets, fluence, dens, spec, kern, stream)
-        sb["batched_speedup"] = value / world / sb["value"]
+        sb["batched_speedup"] = value / sb["value"]
         line["single_beam"] = sb
-        if world == 1:
-            line["reference_cuda"] = reference_cuda_leg(ctx, cfg, bundles, flags, all_beamlets, fluence, dens, spec,
-                                                        stream, value)
+        line["reference_cuda"] = reference_cuda_leg(ctx, cfg, bundles, flags, all_beamlets, fluence, dens, spec,
+                                                    stream, value)
         line["optimizer"] = optimizer_leg(ctx, args.opt_iters, args.opt_rows)
-        if world == 1:
-            line["c4"] = c4_leg(ctx)
+        line["c4"] = c4_leg(ctx)
         # the service's worker contexts start from a device the earlier legs
         # have handed back, as a service process would find it
         import gc

@@ -67,15 +67,20 @@ def test_cccs_matches_oracle(ctx, case_fn, idx):
         assert np.abs(D - Do).max() <= 5e-2 * np.abs(Do).max()
 
 
-def test_cccs_schedules_agree_bitwise(ctx):
+@pytest.mark.parametrize("case_fn", [small_case, c1_case], ids=["8x8", "16x16"])
+def test_cccs_schedules_agree_bitwise(ctx, case_fn):
+    """One block per beamlet and one block per (beamlet, zenith bin): the same
+    matrix, bit for bit (the 8x8 map with 4x4 cones, and the 16x16 march with
+    the 8x6 kernel)."""
     import torch
 
-    case = small_case()
+    case = case_fn()
     dens, sp, kn, _, _ = _setup(ctx, case)
     res = []
     for sched in (0, 1):
         m = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn, cccs_schedule=sched)
         res.append(m.to_host())
+        m.close()
     torch.cuda.synchronize()
     for a, b in zip(*res):
         np.testing.assert_array_equal(a, b)
