@@ -339,7 +339,7 @@ def beamletFlagInit(ctx, bundles, ptv_mask, volume, super_sampling=3):
 class _Params(C.Structure):
     _fields_ = [("extent", C.c_float), ("ss_factor", C.c_int), ("value_type", C.c_int), ("cccs_schedule", C.c_int),
                 ("batch_beamlets", C.c_uint64), ("memory_budget", C.c_uint64), ("verbose", C.c_int),
-                ("host_out", C.c_void_p), ("graph", C.c_int)]
+                ("host_out", C.c_void_p), ("graph", C.c_int), ("overlap", C.c_int)]
 
 
 class _HostCSR(C.Structure):
@@ -462,12 +462,14 @@ class MatCSREnsemble:
 
 def DoseMatConstruction(ctx, beamlets_per_beam, fluence, density, spectrum, kernel, extent=2.0, ss_factor=5,
                         value_type="f32", cccs_schedule=-1, memory_budget=0, batch_beamlets=0, verbose=False,
-                        stream=None, host_out=None, graph=False):
+                        stream=None, host_out=None, graph=False, overlap=True):
     """IMRT::DoseMatConstruction: `beamlets_per_beam` is a list of BEAM_DTYPE
     arrays (one per beam).  Returns a MatCSREnsemble.  host_out: a HostCSR
     (of this value type) that receives a host copy of the matrix, batch by
     batch while it is built.  graph: each batch launched as one CUDA graph
-    (kept per batch shape in the context and updated in place)."""
+    (kept per batch shape in the context and updated in place).  overlap: each
+    batch's column stage runs on a second stream beside the next batch's
+    Terma and CCCS (up to twice the BEV scratch); the matrix is the same."""
     counts = np.array([len(b) for b in beamlets_per_beam], np.uint32)
     allb = np.ascontiguousarray(np.concatenate([np.asarray(b, BEAM_DTYPE).reshape(-1) for b in beamlets_per_beam]),
                                 BEAM_DTYPE) if len(beamlets_per_beam) else np.zeros(0, BEAM_DTYPE)
@@ -480,7 +482,8 @@ def DoseMatConstruction(ctx, beamlets_per_beam, fluence, density, spectrum, kern
             raise ValueError(f"host_out holds {host_out.row_off.numel() - 1} rows, the plan has {allb.size}")
         hs = host_out._struct()
     prm = _Params(extent, ss_factor, VALUE_TYPES[value_type], cccs_schedule, batch_beamlets, memory_budget,
-                  int(verbose), C.cast(C.pointer(hs), C.c_void_p) if hs is not None else None, int(bool(graph)))
+                  int(verbose), C.cast(C.pointer(hs), C.c_void_p) if hs is not None else None, int(bool(graph)),
+                  int(bool(overlap)))
     h = C.c_void_p()
     st = ctx.lib.fd2_dose_mat_construct(ctx.h, len(counts), _p(counts), _p(allb), _p(fl), density.h, spectrum.h,
                                         kernel.h, C.byref(prm), C.byref(h),

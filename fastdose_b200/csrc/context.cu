@@ -117,6 +117,7 @@ int fd2_context_destroy(fd2_context* c) {
         cudaStreamSynchronize(c->stream);
         cudaStreamDestroy(c->stream);
     }
+    if (c->aux_stream) cudaStreamDestroy(c->aux_stream);
     if (c->pool) {
         cudaDeviceSynchronize();  // stream-ordered frees on other streams complete first
         cudaMemPoolDestroy(c->pool);

@@ -540,6 +540,7 @@ void fd2_dosemat_params_default(fd2_dosemat_params_t* p) {
     p->verbose = 0;
     p->host_out = nullptr;
     p->graph = 0;
+    p->overlap = 1;
 }
 
 int fd2_bev2pvcs(fd2_context* ctx, const fd2_beam_t* h_beam, const fd2_density* density, const float* d_bev,
@@ -581,6 +582,8 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     FD2_REQUIRE(params.cccs_schedule >= -2 && params.cccs_schedule <= 1, FD2_ERR_INVALID_ARGUMENT,
                 "cccs_schedule %d (-2..1)", params.cccs_schedule);
     FD2_REQUIRE(params.graph == 0 || params.graph == 1, FD2_ERR_INVALID_ARGUMENT, "graph %d (0 or 1)", params.graph);
+    FD2_REQUIRE(params.overlap == 0 || params.overlap == 1, FD2_ERR_INVALID_ARGUMENT, "overlap %d (0 or 1)",
+                params.overlap);
     FD2_REQUIRE(!(params.graph && params.host_out), FD2_ERR_NOT_SUPPORTED,
                 "dose_mat_construct: graph capture and host_out are exclusive");
     cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
@@ -611,19 +614,31 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
     e->n_cols = nvox;
     e->value_type = params.value_type;
     e->mat_rows.assign(1, 0);
-    // Column geometry and candidate counts of every beamlet, before any dose:
-    // their sum bounds the matrix, which is then allocated once.
-    std::vector<ColumnInfo> infos(total);
-    for (size_t k = 0; k < total; k++) make_column_info(beams[k], &vol, infos[k]);
+    // Column geometry and candidate counts of every beamlet, before the first
+    // column stage: their sum bounds the matrix, which is then allocated once.
+    // The geometry goes up and the counts run on stream `s`; the reservation
+    // is enqueued on st.  With the column stage overlapped this runs after the
+    // first batch's Terma and CCCS are enqueued, on the column stream, so the
+    // host work and the count kernel hide behind that batch's march.
+    std::vector<ColumnInfo> infos;
     ColumnInfo* d_infos = nullptr;
     std::vector<uint32_t> cnt;
-    int rc = upload(infos, &d_infos, ctx->pool, st);
-    if (!rc) rc = column_counts(ctx, d_infos, total, vol, params.extent, st, cnt);
-    uint64_t cap_total = 0;
-    for (uint32_t c : cnt) cap_total += c;
-    if (!rc) rc = ensemble_reserve(e, total, cap_total);
     HostSink sink;  // declared before the ensemble is destroyed on any path: its copies finish first
-    if (!rc && params.host_out) rc = sink.init(params.host_out, e);
+    bool columns_ready = false;
+    auto setup_columns = [&](cudaStream_t s) -> int {
+        columns_ready = true;
+        infos.resize(total);
+        for (size_t k = 0; k < total; k++) make_column_info(beams[k], &vol, infos[k]);
+        FD2_TRY(upload(infos, &d_infos, ctx->pool, s));
+        FD2_TRY(column_counts(ctx, d_infos, total, vol, params.extent, s, cnt));
+        uint64_t cap_total = 0;
+        for (uint32_t c : cnt) cap_total += c;
+        FD2_TRY(ensemble_reserve(e, total, cap_total));
+        if (params.host_out) FD2_TRY(sink.init(params.host_out, e));
+        return FD2_OK;
+    };
+    const bool overlap = params.overlap && !params.graph;
+    int rc = overlap ? FD2_OK : setup_columns(st);
     if (rc) {
         if (d_infos) cudaFreeAsync(d_infos, st);
         fd2_csr_ensemble_destroy(e);
@@ -650,6 +665,34 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         const size_t n_batches = std::max<size_t>(1, (all + budget - 1) / std::max<size_t>(budget, 1));
         budget = std::min(budget, (all + n_batches - 1) / n_batches + (size_t)1);
     }
+    // Column stage beside the next batch (params.overlap, direct launches):
+    // batch i fills BEV slot i % 2 on st; its column stage waits for the
+    // batch's CCCS and runs on the context's second stream (cs) while st goes
+    // on with batch i + 1 in the other slot; before batch i + 2 reuses a slot,
+    // st waits for the column stage that read it.
+    cudaStream_t cs = st;
+    cudaEvent_t ev_ready = nullptr, ev_slot[2] = {nullptr, nullptr};
+    bool slot_used[2] = {false, false};
+    if (!rc && overlap) {
+        if (!ctx->aux_stream && cudaStreamCreateWithFlags(&ctx->aux_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            ctx->aux_stream = nullptr;
+            set_error("dose_mat_construct: cannot create the column stream");
+            rc = FD2_ERR_CUDA;
+        }
+        for (cudaEvent_t* ev : {&ev_ready, &ev_slot[0], &ev_slot[1]})
+            if (!rc && cudaEventCreateWithFlags(ev, cudaEventDisableTiming) != cudaSuccess) {
+                set_error("dose_mat_construct: cannot create events");
+                rc = FD2_ERR_CUDA;
+            }
+        if (!rc) cs = ctx->aux_stream;
+        // the column stream starts after everything enqueued on st so far
+        // (the matrix reservation, the column geometry, the fluence)
+        if (!rc && (cudaEventRecord(ev_ready, st) != cudaSuccess || cudaStreamWaitEvent(cs, ev_ready, 0) != cudaSuccess)) {
+            set_error("dose_mat_construct: cannot order the column stream");
+            rc = FD2_ERR_CUDA;
+        }
+    }
+    size_t n_batch = 0;
     size_t b0 = 0, beam0 = 0;
     const auto t_start = std::chrono::steady_clock::now();
     auto ms_since = [&](std::chrono::steady_clock::time_point t) {
@@ -676,8 +719,15 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         // BEV buffers [beamlet][L][P] for Terma, density, dose
         std::vector<size_t> off(nb + 1, 0);
         for (size_t k = 0; k < nb; k++) off[k + 1] = off[k] + (size_t)beams[b0 + k].long_dim * P;
+        const int slot = overlap ? (int)(n_batch & 1) : 0;
+        n_batch++;
+        if (overlap && slot_used[slot] && cudaStreamWaitEvent(st, ev_slot[slot], 0) != cudaSuccess) {
+            set_error("dose_mat_construct: cannot order the BEV buffer reuse");
+            rc = FD2_ERR_CUDA;
+            break;
+        }
         float* d_bev = nullptr;
-        rc = ctx_buffer(ctx, kBufBev, off[nb] * 3 * sizeof(float), st, (void**)&d_bev);
+        rc = ctx_buffer(ctx, slot ? kBufBev2 : kBufBev, off[nb] * 3 * sizeof(float), st, (void**)&d_bev);
         if (rc) break;
         float *dT = d_bev, *dR = d_bev + off[nb], *dD = d_bev + 2 * off[nb];
         if (params.graph) {
@@ -729,18 +779,38 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
                 }
                 t.stop();
             }
-            StageTimer t(ctx, st, FD2_STAGE_COLUMNS);
+            if (overlap) {
+                if (!columns_ready) FD2_TRY(setup_columns(cs));
+                FD2_CHECK_CUDA(cudaEventRecord(ev_ready, st));
+                FD2_CHECK_CUDA(cudaStreamWaitEvent(cs, ev_ready, 0));
+            }
+            StageTimer t(ctx, cs, FD2_STAGE_COLUMNS);
             int r = append_columns(e, d_infos + b0, cnt.data() + b0, nb, (const float* const*)aD, vol,
-                                   params.extent, params.ss_factor, st);
+                                   params.extent, params.ss_factor, cs);
             t.stop();
             return r;
         }();
-        // release batch buffers
-        for (void* p : {(void*)aF, (void*)aT, (void*)aR, (void*)aD, (void*)d_order})  // d_bev is the context's
+        // release batch buffers: the dose pointer table after the column stage
+        // that reads it (on cs), the others after the CCCS (on st); a failed
+        // batch drains both streams first
+        if (rc && overlap) {
+            cudaStreamSynchronize(st);
+            cudaStreamSynchronize(cs);
+        }
+        for (void* p : {(void*)aF, (void*)aT, (void*)aR, (void*)d_order})  // d_bev is the context's
             if (p) cudaFreeAsync(p, st);
+        if (aD) cudaFreeAsync(aD, cs);
         if (rc) break;
+        if (overlap) {
+            if (cudaEventRecord(ev_slot[slot], cs) != cudaSuccess) {
+                set_error("dose_mat_construct: cannot record the column stage");
+                rc = FD2_ERR_CUDA;
+                break;
+            }
+            slot_used[slot] = true;
+        }
         if (params.host_out) {
-            rc = sink.batch_done(e->n_rows - nb, e->n_rows, st);
+            rc = sink.batch_done(e->n_rows - nb, e->n_rows, cs);
             if (rc) break;
         }
         // per-beam row boundaries
@@ -755,11 +825,26 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
         b0 = b1;
         beam0 = beam1;
     }
+    // a plan without beamlets still gets its (empty) matrix
+    if (!rc && !columns_ready) rc = setup_columns(st);
+    if (overlap && cs != st) {
+        // st resumes after the last column stage; on an error path the host
+        // waits for the column stream instead
+        if (cudaEventRecord(ev_ready, cs) != cudaSuccess || cudaStreamWaitEvent(st, ev_ready, 0) != cudaSuccess) {
+            cudaStreamSynchronize(cs);
+            if (!rc) {
+                set_error("dose_mat_construct: cannot join the column stream");
+                rc = FD2_ERR_CUDA;
+            }
+        }
+    }
     if (d_fluence) cudaFreeAsync(d_fluence, st);
     if (d_beams) cudaFreeAsync(d_beams, st);
     if (d_infos) cudaFreeAsync(d_infos, st);
     if (!rc) rc = ensemble_sync_nnz(e);  // the one wait of the construction, besides the candidate counts
     cudaStreamSynchronize(st);
+    for (cudaEvent_t ev : {ev_ready, ev_slot[0], ev_slot[1]})
+        if (ev) cudaEventDestroy(ev);
     if (!rc && params.host_out) rc = sink.finish();
     if (!rc) {
         fd2::DeviceStatus ds;

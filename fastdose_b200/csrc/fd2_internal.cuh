@@ -62,9 +62,12 @@ struct fd2_context {
     cudaStream_t stream = nullptr;          // internal work stream
     fd2::DeviceStatus* d_status = nullptr;  // device status word
     // reusable grow-only device buffers (fd2::ctx_buffer slots), kept between calls
-    void* buf[4] = {nullptr, nullptr, nullptr, nullptr};
-    size_t buf_bytes[4] = {0, 0, 0, 0};
-    cudaStream_t buf_stream[4] = {nullptr, nullptr, nullptr, nullptr};  // stream of each buffer's last use
+    void* buf[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    size_t buf_bytes[5] = {0, 0, 0, 0, 0};
+    cudaStream_t buf_stream[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // stream of each buffer's last use
+    // second work stream of the construction: the column stage of one batch
+    // runs on it beside the next batch's Terma and CCCS (created on first use)
+    cudaStream_t aux_stream = nullptr;
     // stream-ordered pool for batch buffers and dose-matrix storage; it keeps
     // freed memory (release threshold = max) so repeated plans reuse it
     cudaMemPool_t pool = nullptr;
@@ -147,7 +150,7 @@ namespace fd2 {
 // (calls on one context are serialised: one host thread, work in stream
 // order); growing it replaces the old one in the order of stream `st`, and
 // waits for the device only when the previous use was on another stream.
-enum CtxBuffer { kBufCccs = 0, kBufBev = 1, kBufColumns = 2, kBufBatch = 3, kBufCount = 4 };
+enum CtxBuffer { kBufCccs = 0, kBufBev = 1, kBufColumns = 2, kBufBatch = 3, kBufBev2 = 4, kBufCount = 5 };
 int ctx_buffer(fd2_context* ctx, int slot, size_t bytes, cudaStream_t st, void** out);
 inline int ctx_scratch(fd2_context* ctx, size_t bytes, cudaStream_t st, void** out) {
     return ctx_buffer(ctx, kBufCccs, bytes, st, out);

@@ -241,6 +241,9 @@ int fd2_service_submit(fd2_service* s, const fd2_plan_request_t* q, uint64_t* ti
     r->params = q->params;
     r->params.memory_budget = s->bev_budget;
     r->params.host_out = nullptr;  // a served request's result stays on the device
+    // the admission estimate counts one BEV batch per request, so a worker
+    // builds with one BEV buffer: no column-stage overlap
+    r->params.overlap = 0;
     // a request's latency must not carry a timing run of both CCCS schedules
     // (each new batch shape would add one): served requests take the rule
     if (r->params.cccs_schedule == -1) r->params.cccs_schedule = -2;

@@ -76,6 +76,12 @@ typedef struct fd2_dosemat_params {
                                    place with the next batch's parameters.  The CCCS schedule is
                                    then fixed per batch (-1 acts as -2), and the matrix is bit for
                                    bit the one direct launches give.  fd2_dose_mat_construct only. */
+    int overlap;                /* 1 (default): the column stage of each batch runs on a second stream
+                                   of the context beside the next batch's Terma and CCCS, which then
+                                   fill a second BEV buffer (a plan of several batches holds up to
+                                   twice memory_budget of BEV scratch); 0: one stream, one buffer.
+                                   The matrix is the same bit for bit.  Ignored with graph = 1.
+                                   fd2_dose_mat_construct only. */
 } fd2_dosemat_params_t;
 
 void fd2_dosemat_params_default(fd2_dosemat_params_t* p);

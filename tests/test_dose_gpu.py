@@ -357,6 +357,27 @@ def test_host_copy_while_building(ctx, vt):
         mm.close()
 
 
+@pytest.mark.parametrize("vt", ["f32", "f16"])
+def test_overlapped_column_stage_matches_one_stream(ctx, vt):
+    """The column stage of each batch on the context's second stream, beside
+    the next batch's Terma and CCCS in the other BEV buffer (the default), and
+    the whole construction on one stream: the same matrix, bit for bit, for
+    one batch and for several (batches of 10, 20 and 30 beamlets, so BEV
+    buffers are reused and regrown while a column stage may still read them)."""
+    case = c1_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    beams = [case["beams"][i:i + 10] for i in range(0, len(case["beams"]), 10)]
+    ref = api.DoseMatConstruction(ctx, beams, case["fluence"], dens, sp, kn, value_type=vt, overlap=False)
+    ref_h = ref.to_host()
+    for batch in (0, 30, 10, 20):
+        m = api.DoseMatConstruction(ctx, beams, case["fluence"], dens, sp, kn, value_type=vt, batch_beamlets=batch)
+        for a, b in zip(m.to_host(), ref_h):
+            np.testing.assert_array_equal(a, b)
+        np.testing.assert_array_equal(m.mat_rows(), ref.mat_rows())
+        m.close()
+    ref.close()
+
+
 def _write_folder(path, mats, vals_dtype=np.float32):
     """A doseMatFolder (the reference's layout) from host CSR matrices."""
     path.mkdir(parents=True, exist_ok=True)
