@@ -378,6 +378,38 @@ def test_overlapped_column_stage_matches_one_stream(ctx, vt):
     ref.close()
 
 
+def test_construction_with_empty_beams(ctx):
+    """Beams without beamlets (a beam whose flags are all off) anywhere in the
+    plan add no rows and repeat their neighbour's row boundary; the rows are
+    those of the plan without them, bit for bit, with and without the column
+    overlap and over several batchings.  A plan of empty beams only gives an
+    empty matrix."""
+    from fastdose_b200.types import BEAM_DTYPE
+
+    case = c1_case()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    b = case["beams"]
+    empty = np.zeros(0, BEAM_DTYPE)
+    ref = api.DoseMatConstruction(ctx, [b[:30], b[30:]], case["fluence"], dens, sp, kn)
+    ref_h = ref.to_host()
+    plan = [empty, b[:30], empty, empty, b[30:], empty]
+    for overlap in (True, False):
+        for batch in (0, 16):
+            m = api.DoseMatConstruction(ctx, plan, case["fluence"], dens, sp, kn, overlap=overlap,
+                                        batch_beamlets=batch)
+            for x, y in zip(m.to_host(), ref_h):
+                np.testing.assert_array_equal(x, y)
+            np.testing.assert_array_equal(m.mat_rows(), [0, 0, 30, 30, 30, 100, 100])
+            m.close()
+    for overlap in (True, False):
+        z = api.DoseMatConstruction(ctx, [empty, empty], case["fluence"], dens, sp, kn, overlap=overlap)
+        ro, col, val = z.to_host()
+        assert z.info()["nnz"] == 0 and len(col) == 0 and ro.tolist() == [0]
+        np.testing.assert_array_equal(z.mat_rows(), [0, 0, 0])
+        z.close()
+    ref.close()
+
+
 def _write_folder(path, mats, vals_dtype=np.float32):
     """A doseMatFolder (the reference's layout) from host CSR matrices."""
     path.mkdir(parents=True, exist_ok=True)
