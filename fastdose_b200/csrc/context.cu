@@ -1,5 +1,6 @@
 // context.cu -- context, density, spectrum and CCCS-kernel handles.
 #include <cstring>
+#include <mutex>
 
 #include "fd2_internal.cuh"
 
@@ -40,6 +41,34 @@ void ctx_graphs_free(fd2_context* ctx) {
     }
 }
 
+// One pool per device for the densities of fd2_density_create: created on
+// first use and kept until the process ends, so a density may be freed after
+// the context it was made with; freed memory is kept for the next density.
+int density_pool(int device, cudaMemPool_t* out) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[kMaxDevices] = {};
+    FD2_REQUIRE(device >= 0 && device < kMaxDevices, FD2_ERR_INVALID_ARGUMENT, "density pool: device %d", device);
+    std::lock_guard<std::mutex> lock(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps pp = {};
+        pp.allocType = cudaMemAllocationTypePinned;
+        pp.handleTypes = cudaMemHandleTypeNone;
+        pp.location.type = cudaMemLocationTypeDevice;
+        pp.location.id = device;
+        const uint64_t keep = ~0ull;
+        cudaMemPool_t p = nullptr;
+        FD2_CHECK_CUDA(cudaMemPoolCreate(&p, &pp));
+        if (cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, (void*)&keep) != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            fd2::set_error("density pool: cannot set its release threshold");
+            return FD2_ERR_CUDA;
+        }
+        pools[device] = p;
+    }
+    *out = pools[device];
+    return FD2_OK;
+}
+
 int density_create_pooled(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume,
                           fd2_density** out) {
     FD2_REQUIRE(ctx && host_density && volume && out, FD2_ERR_INVALID_ARGUMENT, "density_create: null argument");
@@ -58,6 +87,7 @@ int density_create_pooled(fd2_context* ctx, const float* host_density, const fd2
     d->ctx = ctx;
     d->vol = *volume;
     d->d_density = (float*)p;
+    d->device = ctx->device;
     d->pooled = true;
     *out = d;
     return FD2_OK;
@@ -193,20 +223,30 @@ int fd2_density_create(fd2_context* ctx, const float* host_density, const fd2_vo
     FD2_REQUIRE(nv > 0, FD2_ERR_INVALID_ARGUMENT, "density_create: empty volume");
     FD2_REQUIRE(volume->voxel_size[0] > 0 && volume->voxel_size[1] > 0 && volume->voxel_size[2] > 0,
                 FD2_ERR_INVALID_ARGUMENT, "density_create: voxel size must be positive");
-    auto* d = new fd2_density();
-    d->ctx = ctx;
-    d->vol = *volume;
-    if (cudaMalloc(&d->d_density, nv * sizeof(float)) != cudaSuccess) {
-        delete d;
-        fd2::set_error("density_create: cudaMalloc of %zu bytes failed", nv * sizeof(float));
+    // The device copy comes from the library's density pool of this device
+    // (no cudaMalloc / cudaFree per plan: those driver calls now and then took
+    // tens to hundreds of ms), and is complete when this returns, so any
+    // stream may read it.
+    cudaMemPool_t pool = nullptr;
+    FD2_TRY(fd2::density_pool(ctx->device, &pool));
+    void* p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, nv * sizeof(float), pool, ctx->stream) != cudaSuccess) {
+        cudaGetLastError();
+        fd2::set_error("density_create: allocation of %zu bytes failed", nv * sizeof(float));
         return FD2_ERR_OUT_OF_MEMORY;
     }
-    if (cudaMemcpy(d->d_density, host_density, nv * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
-        cudaFree(d->d_density);
-        delete d;
+    if (cudaMemcpyAsync(p, host_density, nv * sizeof(float), cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess ||
+        cudaStreamSynchronize(ctx->stream) != cudaSuccess) {
+        cudaFreeAsync(p, ctx->stream);
+        cudaStreamSynchronize(ctx->stream);
         fd2::set_error("density_create: copy failed");
         return FD2_ERR_CUDA;
     }
+    auto* d = new fd2_density();
+    d->ctx = ctx;
+    d->vol = *volume;
+    d->d_density = (float*)p;
+    d->device = ctx->device;
     *out = d;
     return FD2_OK;
 }
@@ -214,10 +254,21 @@ int fd2_density_create(fd2_context* ctx, const float* host_density, const fd2_vo
 int fd2_density_destroy(fd2_density* d) {
     if (!d) return FD2_OK;
     if (d->d_density) {
-        if (d->pooled)
+        if (d->pooled) {
             cudaFreeAsync(d->d_density, d->ctx->stream);
-        else
-            cudaFree(d->d_density);
+        } else {
+            // A density made by fd2_density_create may be read by work on any
+            // stream, and may outlive its context: like cudaFree, wait for the
+            // device, then return the memory to the library's density pool,
+            // which lives as long as the process, on the default stream.
+            int cur = -1;
+            cudaGetDevice(&cur);
+            if (cur != d->device) cudaSetDevice(d->device);
+            cudaDeviceSynchronize();
+            cudaFreeAsync(d->d_density, cudaStreamLegacy);
+            cudaGetLastError();  // nothing a later launch check should see
+            if (cur >= 0 && cur != d->device) cudaSetDevice(cur);
+        }
     }
     delete d;
     return FD2_OK;

@@ -123,8 +123,9 @@ struct StageTimer {
 struct fd2_density {
     fd2_context* ctx = nullptr;
     fd2_volume_t vol{};
-    float* d_density = nullptr;  // float[z][y][x]
-    bool pooled = false;         // from the context's pool in its stream's order (density_create_pooled)
+    float* d_density = nullptr;  // float[z][y][x], from the context's pool
+    int device = 0;
+    bool pooled = false;         // a service density: used and freed in the context stream's order only
 };
 
 struct fd2_spectrum {
@@ -160,6 +161,8 @@ inline int ctx_scratch(fd2_context* ctx, size_t bytes, cudaStream_t st, void** o
 // the context's stream, and returns to it the same way on destroy: no call
 // that waits for the whole device.  Only for work issued on ctx->stream (a
 // service worker's requests); the public fd2_density_create allocates plainly.
+constexpr int kMaxDevices = 64;
+int density_pool(int device, cudaMemPool_t* out);
 int density_create_pooled(fd2_context* ctx, const float* host_density, const fd2_volume_t* volume,
                           fd2_density** out);
 

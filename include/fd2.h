@@ -190,7 +190,11 @@ int fd2_context_graph_counts(fd2_context* ctx, uint64_t* launches, uint64_t* ins
 /*
  * fastdose::density_h2d (FastDoseLib/src/density.cu:23-58).  Copies a host
  * density volume to the device.  Sampling is trilinear on texel centres i+0.5
- * with zero outside the volume (the reference's linear/border texture).
+ * with zero outside the volume (the reference's linear/border texture).  The
+ * device copy comes from a memory pool the library keeps per device for the
+ * life of the process, and is complete on return; fd2_density_destroy waits
+ * for the device (as cudaFree does) and returns it to that pool.  A density
+ * may be destroyed after its context.
  */
 int fd2_density_create(fd2_context* ctx, const float* host_density,
                        const fd2_volume_t* volume, fd2_density** out);

@@ -410,6 +410,24 @@ def test_construction_with_empty_beams(ctx):
     ref.close()
 
 
+def test_density_outlives_its_context(ctx):
+    """A density is freed after its context was destroyed (the Python objects
+    of a caller can go in any order): no error, and later work on another
+    context is unaffected."""
+    import torch
+
+    case = small_case()
+    c2 = api.Context(0)
+    d2 = api.Density(c2, case["phantom"].density, case["phantom"].volume)
+    c2.close()
+    d2.close()
+    dens, sp, kn, _, _ = _setup(ctx, case)
+    m = api.DoseMatConstruction(ctx, [case["beams"]], case["fluence"], dens, sp, kn)
+    torch.cuda.synchronize()
+    assert m.info()["nnz"] > 0
+    m.close()
+
+
 def _write_folder(path, mats, vals_dtype=np.float32):
     """A doseMatFolder (the reference's layout) from host CSR matrices."""
     path.mkdir(parents=True, exist_ok=True)
