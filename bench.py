@@ -911,6 +911,66 @@ def reference_cuda_leg(ctx, cfg, bundles, flags, all_beamlets, fluence, dens, sp
     return out
 
 
+def c1_leg(ctx, stream, reps=20):
+    """C1, plain CCCS of one beam: the 64^3 slab phantom, gantry 0, 10x10 open
+    beamlets of 0.5 cm (16x16 sub-maps).  This library's whole construction
+    (Terma, CCCS, columns) per plan with the plan's 8x6 cones and with 8x8,
+    CUDA events over `reps` plans; beside it the reference's own CUDA build
+    (oracle/_ref/libfdref.so) running IMRT::DoseMatConstruction's per-beam
+    steps on the same beam with the 8x8 kernel (its 8x6 march never ends).
+    A baseline leg: nothing here is this library's product path."""
+    import torch
+
+    from fastdose_b200 import api, phantoms
+    from fastdose_b200.types import make_bundle
+
+    cfg = phantoms.config1()
+    ph = cfg["phantom"]
+    bund = make_bundle(cfg["isocenter"], cfg["angles"][0], sad=cfg["sad"], fluence_dim=cfg["fluence_dim"],
+                       beamlet_size=cfg["beamlet_size"], sub_fluence_dim=cfg["sub_fluence_dim"],
+                       sub_fluence_on=cfg["sub_fluence_on"], long_spacing=cfg["long_spacing"])
+    flags = np.ones(cfg["fluence_dim"] ** 2, np.uint8)
+    beams = api.bundle_beamlets(bund, flags, ph.volume)
+    fluence = api.beamlet_fluence(bund)
+    dens, spec = api.Density(ctx, ph.density, ph.volume), api.Spectrum(ctx, cfg["spectrum"])
+    k88 = phantoms.synthetic_kernel(n_theta=8, n_phi=8)
+    out = {"workload": "64^3 slab phantom at 2.5 mm (bone and lung slabs), one beam at gantry 0, 10x10 open "
+                       "beamlets of 0.5 cm, 16x16 sub-maps, 12-bin spectrum", "beamlets": int(len(beams))}
+    for name, kern in (("8x6", cfg["kernel"]), ("8x8", k88)):
+        kn = api.Kernel(ctx, kern)
+        for _ in range(3):
+            api.DoseMatConstruction(ctx, [beams], fluence, dens, spec, kn, stream=stream).close()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            api.DoseMatConstruction(ctx, [beams], fluence, dens, spec, kn, stream=stream).close()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        out[f"fd2_{name}"] = {"ms_per_plan": ms, "beamlets_per_s": len(beams) / (ms * 1e-3)}
+    from oracle import ref
+
+    if not ref.available():
+        out["reference_8x8"] = {"unavailable": "oracle/_ref/libfdref.so is not built"}
+        return out
+    runs = []
+    for _ in range(4):
+        r = ref.dose_mat_steps(np.array([bund]), flags.reshape(1, -1), ph.density, ph.volume, cfg["spectrum"], k88,
+                               extent=cfg["extent"])
+        if r["status"] != 0:
+            out["reference_8x8"] = {"unavailable": f"reference DoseMatConstruction steps returned {r['status']}"}
+            return out
+        runs.append([float(x) for x in r["times_ms"]])
+    t = min(runs[1:], key=lambda x: x[4])  # the first run warms the reference's code path
+    out["reference_8x8"] = {"ms_per_plan": t[4], "beamlets_per_s": r["beamlets"] / (t[4] * 1e-3),
+                            "stage_ms": {"terma": t[0], "cccs": t[1], "interp": t[2], "dense_to_csr": t[3]},
+                            "note": "IMRTDoseMat.cu:183-259 run step by step by oracle/ref/ref_harness.cu; the "
+                                    "fastest of three runs after one warm-up"}
+    out["speedup_vs_reference_8x8"] = out["fd2_8x8"]["beamlets_per_s"] / out["reference_8x8"]["beamlets_per_s"]
+    return out
+
+
 def run_fd2(args, rank, world):
     import torch
     import torch.distributed as dist
@@ -1104,6 +1164,7 @@ def run_fd2(args, rank, world):
         line["single_beam"] = sb
         line["reference_cuda"] = reference_cuda_leg(ctx, cfg, bundles, flags, all_beamlets, fluence, dens, spec,
                                                     stream, value)
+        line["c1"] = c1_leg(ctx, stream)
         line["optimizer"] = optimizer_leg(ctx, args.opt_iters, args.opt_rows)
         line["c4"] = c4_leg(ctx)
         # the service's worker contexts start from a device the earlier legs
@@ -1135,6 +1196,7 @@ def main():
     ap.add_argument("--opt-iters", type=int, default=500)
     ap.add_argument("--opt-rows", type=int, default=2_500_000)
     ap.add_argument("--only-optimizer", action="store_true", help="run the optimizer leg alone (profiling)")
+    ap.add_argument("--only-c1", action="store_true", help="time config 1 (one beam, 64^3) alone")
     ap.add_argument("--only-spmv", default=None, choices=["f32_i32", "f32_packed16", "f16_packed16", "bf16_packed16"],
                     help="time A x and A^T y of the optimization matrix in one format (profiling)")
     ap.add_argument("--spmv-reps", type=int, default=10)
@@ -1156,6 +1218,13 @@ def main():
 
         torch.cuda.set_device(0)
         print(json.dumps({"c4": c4_leg(api.Context(0))}), flush=True)
+        return
+    if args.only_c1:
+        import torch
+
+        from fastdose_b200 import api
+
+        print(json.dumps({"c1": c1_leg(api.Context(0), torch.cuda.current_stream())}), flush=True)
         return
     if args.only_spmv:
         import torch
