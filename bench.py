@@ -38,8 +38,8 @@ METRIC = "CCCS beamlets/s (dose-loading matrix, batched 4pi)"
 # From one ncu capture of the CCCS march on the 40-beam plan (6056 beamlets,
 # 8.2 waves; profiles/cccs_kernel_4pi_torso_40beams.md):
 # dram__bytes_read.sum + dram__bytes_write.sum, and smsp__inst_executed.sum
-CCCS_DRAM_BYTES_PER_BEAMLET = (28.925890e9 + 9.509276e9) / 6056
-CCCS_WARP_INST_PER_BEAMLET = 141.212517619e9 / 6056
+CCCS_DRAM_BYTES_PER_BEAMLET = (28.562879e9 + 9.447058e9) / 6056
+CCCS_WARP_INST_PER_BEAMLET = 124.063924973e9 / 6056
 UNIT = "beamlets/s"
 
 
@@ -1086,7 +1086,7 @@ def run_fd2(args, rank, world):
     L = np.concatenate([b["long_dim"] for b in beamlets]).astype(np.float64)
     cccs_bytes = float(np.sum(4.0 * P * L * 3))  # Terma + density read, dose written, per beamlet
     # DRAM bytes the CCCS kernel moves per beamlet: dram__bytes_read.sum + dram__bytes_write.sum of one
-    # ncu capture of the march on the 40-beam plan (6056 beamlets, 38.4 GB),
+    # ncu capture of the march on the 40-beam plan (6056 beamlets, 38.0 GB),
     # scaled by the beamlets of this step (each zenith pass re-reads its slices: traffic grows with beamlets)
     cccs_traffic = CCCS_DRAM_BYTES_PER_BEAMLET * n_bl
     cccs_ms = stages["cccs"]

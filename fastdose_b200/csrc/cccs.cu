@@ -43,9 +43,10 @@ namespace fd2 {
 namespace {
 
 constexpr int kStepCap = 1 << 20;  // per-slice step cap (the watchdog bound)
-// The 16x16 march is compiled for at most 8 azimuth warps (register budget
-// for 4 such blocks of 256 threads, i.e. 5 blocks of 192 threads, per SM;
-// measured faster than 48 registers at 7 blocks of 192).
+// The 16x16 march is compiled for at most 8 azimuth warps, with the register
+// budget of 3 such blocks of 256 threads per SM: 80 registers, 4 blocks of
+// 192 threads (6 azimuths).  On the 4pi plan that measured faster than 48,
+// 64, 72, 96 and 126 registers (7, 5, 4, 3 and 2 blocks of 192).
 constexpr int kFx16Threads = 256;
 
 struct RayGeom {  // per-beamlet scalars the march needs
@@ -190,7 +191,7 @@ __device__ __forceinline__ float seg_length(float l2) {
 // RPL >= ceil(F / k).
 template <int RPL, bool kFx16, bool kCols = false, bool kTab = false>
 __global__ void __launch_bounds__(kFx16 || kCols || kTab ? kFx16Threads : 768,
-                                  kFx16 ? 4 : ((kCols || kTab) && RPL <= 8 ? 4 : (kCols || kTab ? 3 : 1)))
+                                  kFx16 ? 3 : ((kCols || kTab) && RPL <= 8 ? 4 : (kCols || kTab ? 3 : 1)))
     cccs_kernel(const fd2_beam_t* __restrict__ beams,
                                                    const float* const* __restrict__ terma,
                                                    const float* const* __restrict__ dens,
