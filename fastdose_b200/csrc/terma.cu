@@ -59,8 +59,11 @@ __device__ __forceinline__ float3 bev_to_pvcs(float3 v, float th, float ph, floa
                        k * cr + ct * t.z + st * (sr * t.y));
 }
 
+// 40 registers, 6 blocks per SM: the ray trace waits on density reads, and
+// the extra warps hide more of that latency (measured 66.6 against 68.7 ms per
+// 400-beam plan at 48 registers; 32 registers spilled and was slower).
 template <bool kSkipDark>
-__global__ void __launch_bounds__(256) terma_kernel(const fd2_beam_t* __restrict__ beams,
+__global__ void __launch_bounds__(256, 6) terma_kernel(const fd2_beam_t* __restrict__ beams,
                                                     const float* const* __restrict__ fluence,
                                                     float* const* __restrict__ terma, float* const* __restrict__ dens,
                                                     const float* __restrict__ density, int nx, int ny, int nz,
