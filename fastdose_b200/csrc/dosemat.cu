@@ -686,7 +686,7 @@ int fd2_dose_mat_construct(fd2_context* ctx, size_t n_beams, const uint32_t* n_p
             }
         if (!rc) cs = ctx->aux_stream;
         // the column stream starts after everything enqueued on st so far
-        // (the matrix reservation, the column geometry, the fluence)
+        // (the fluence and beamlet uploads)
         if (!rc && (cudaEventRecord(ev_ready, st) != cudaSuccess || cudaStreamWaitEvent(cs, ev_ready, 0) != cudaSuccess)) {
             set_error("dose_mat_construct: cannot order the column stream");
             rc = FD2_ERR_CUDA;
