@@ -577,10 +577,12 @@ def c4_leg(ctx, n_per_iso=300, opt_iters=20):
     n_bl = sum(len(b) for p in plans for b in p["beams"])
     counts = [len(b) for p in plans for b in p["beams"]]
     s = torch.cuda.current_stream()
-    # warm-up: the four matrices once, untimed (the CCCS schedule of each batch
-    # shape is tuned and the context's buffers reach their size), then timed
-    for p in plans:
-        api.DoseMatConstruction(ctx, p["beams"], p["fluence"], dens, spec, kern, stream=s).close()
+    # warm-up: the four matrices once, untimed and held together as the timed
+    # pass holds them (the CCCS schedule of each batch shape is tuned, and the
+    # context's buffers and memory pool reach their size), then timed
+    warm = [api.DoseMatConstruction(ctx, p["beams"], p["fluence"], dens, spec, kern, stream=s) for p in plans]
+    for m in warm:
+        m.close()
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(len(plans) + 1)]
     ev[0].record(s)
